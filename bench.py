@@ -1,0 +1,381 @@
+#!/usr/bin/env python3
+"""Benchmark: polyenergetic cone-beam forward projection on B200.
+
+Workload (default): two-material polyenergetic projection with a focused
+anti-scatter grid and scintillator response -- 256^3 soft-tissue + bone density
+maps at 0.5 mm, 360 views, 512 x 384 detector at 0.8 mm, 120 kVp in 1-keV bins
+20-120 keV (101 bins), SOD 1000 / SDD 1500 mm, grid 10:1 at 40 lines/cm with
+per-pixel per-energy transmission.  A step is one full forward projection
+(all 70.8 M rays).  Synthetic seeded phantom.
+
+  value  rays/s with inputs resident in HBM (CUDA events, L2 flushed between steps)
+  e2e    rays/s through ctfp_forward_host: host volumes in, host I/IAbsorb out
+  roofline  the march kernel against the measured HBM copy bandwidth, with
+            32 B (8 FP32 corners) per voxel-sample of algorithmic traffic
+  cpu_baseline  the FP64 oracle on the host cores over a seeded ray subset
+
+Multi-GPU (torchrun): every rank projects its own seeded object (independent
+objects, weak scaling, no data-path collective); time is the max over ranks.
+--impl reference runs the reference's own implementation of the path (see
+reference_arm below).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+BYTES_PER_VOXEL_SAMPLE = 32  # 8 FP32 corners, the reuse-free trilinear footprint
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ctfp_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        if torch.cuda.is_available():
+            torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier_sync(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(w, gpu_I, budget_s: float):
+    """FP64 oracle over a seeded subset of rays on all host cores; also the
+    max relative error of the GPU result on those rays."""
+    from oracle import oracle as O
+    from ct_forward_projection_b200.projector import Projector  # noqa: F401  (tables below)
+    g = w.geometry
+    n_rays = w.n_rays
+    rng = np.random.RandomState(7)
+    vols = [v.cpu().numpy() for v in w._vols]
+    W = w._W
+    mu = w.mu_table()
+    # calibrate on a small subset, then size the sample to the budget
+    ids = np.sort(rng.choice(n_rays, 512, replace=False))
+    t0 = time.perf_counter()
+    O.forward(g, vols, mu, W, O.TRILINEAR, ids)
+    dt = time.perf_counter() - t0
+    n = int(min(n_rays, max(512, 512 * budget_s / max(dt, 1e-6))))
+    ids = np.sort(rng.choice(n_rays, n, replace=False))
+    t0 = time.perf_counter()
+    ref = O.forward(g, vols, mu, W, O.TRILINEAR, ids)
+    dt = time.perf_counter() - t0
+    got = gpu_I.reshape(-1)[ids].astype(np.float64)
+    err = float(np.max(np.abs(got - ref["I"]) / np.maximum(np.abs(ref["I"]), 1e-30)))
+    return {"value": n / dt, "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n} seeded random rays (seed 7) of the full workload, FP64 oracle, {dt:.1f} s"}, err
+
+
+def reference_arm(args, w, ws, rank):
+    """The reference's own implementation of the path.  Its projector is CUDA
+    (Source/CUDAFun/CBCTPolyProjGPU.cu); oracle/build_ref.sh builds it from the
+    reference sources into oracle/_ref/ctfp_ref.  When that binary is absent the
+    oracle port on the host cores stands in."""
+    if rank != 0:
+        return None
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ctfp_ref")
+    if os.path.exists(ref_bin):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import ref_runner
+        return ref_runner.bench_line(args, w)
+    from oracle import oracle as O
+    g = w.geometry
+    rng = np.random.RandomState(7)
+    mu = w.mu_table()
+    vals = []
+    vols = [v.cpu().numpy() for v in w._vols]
+    n = 4096
+    for s in range(args.warmup + args.steps):
+        ids = np.sort(rng.choice(w.n_rays, n, replace=False))
+        t0 = time.perf_counter()
+        O.forward(g, vols, mu, w._W, O.TRILINEAR, ids)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            vals.append(n / dt)
+    v = statistics.mean(vals)
+    return {"impl": "reference", "metric": "rays/s (forward projection)", "value": v, "unit": "rays/s",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "config": {"workload": w.name}, "dtype": "f64",
+            "cpu_baseline": {"value": v, "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{n} seeded random rays per step"},
+            "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poly_grid_256")
+    ap.add_argument("--interp", default="trilinear", choices=["trilinear", "texemu", "texture"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+
+    from ct_forward_projection_b200 import physics
+    from ct_forward_projection_b200.projector import Projector
+
+    ws, rank, local = dist_setup(args.gpus)
+    w = physics.workload(args.workload)
+    w.seed += rank  # each rank projects its own object
+    dev = f"cuda:{local}"
+
+    if args.impl == "reference":
+        w._vols = physics.phantom(w, "cpu")
+        from oracle import oracle as O
+        pr_tmp = None
+        # energy weights for the oracle, built through the library's table builders
+        pr_tmp = Projector(w.geometry, len(w.materials), "trilinear", local)
+        pr_tmp.set_tables_from_workload(w)
+        w._W = _weights_from_tables(w, local)
+        pr_tmp.close()
+        line = reference_arm(args, w, ws, rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    vols = physics.phantom(w, dev)
+    M = len(vols)
+    pr = Projector(w.geometry, M, args.interp, local)
+    pr.set_tables_from_workload(w)
+    P, V, U = pr.shape_proj
+    rays = P * U * V
+    out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    # ---------------- device-resident forward (value) -----------------------
+    for _ in range(args.warmup):
+        pr.forward(vols, out=out)
+    barrier_sync(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier_sync(ws)
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        ev[s][0].record(stream)
+        pr.forward(vols, out=out)
+        ev[s][1].record(stream)
+    barrier_sync(ws)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = max_over_ranks(statistics.mean(step_ms), ws)
+    value = ws * rays / (ms / 1e3)
+
+    # roofline: algorithmic bytes of the dominant kernel per launch
+    support = pr.count_support_samples()
+    vs_launch = support * M
+    nominal_vs = M * rays * int(pr.info["intNum"])
+    peak, peak_kind = measured_peak_hbm()
+    achieved = vs_launch * BYTES_PER_VOXEL_SAMPLE / (ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": peak_kind,
+                "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_launch / (ms / 1e3),
+                "nominal_voxel_samples_per_launch": nominal_vs,
+                "note": "achieved = 32 B x support voxel-samples / kernel time; traffic from ncu in profiles/"}
+
+    # ---------------- end to end through ctfp_forward_host (e2e) ------------
+    e2e = None
+    if not args.no_e2e:
+        host_vols = [v.cpu().pin_memory() for v in vols]
+        host_out = {"I": torch.empty((P, V, U)).pin_memory(), "IAbsorb": torch.empty((P, V, U)).pin_memory(),
+                    "I0": torch.empty((V, U)).pin_memory()}
+        for _ in range(2):
+            pr.forward_host(host_vols, out=host_out)
+        barrier_sync(ws)
+        t_e2e = []
+        for s in range(args.steps):
+            t0 = time.perf_counter()
+            pr.forward_host(host_vols, out=host_out)
+            t_e2e.append(time.perf_counter() - t0)
+        barrier_sync(ws)
+        e2e_s = max_over_ranks(statistics.mean(t_e2e), ws)
+        h2d = sum(v.numel() * 4 for v in host_vols)
+        d2h = 2 * rays * 4 + U * V * 4
+        e2e = {"value": ws * rays / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "s_per_step": e2e_s}
+
+    # ---------------- forward + adjoint (extra) -----------------------------
+    fa = None
+    if not args.no_adjoint:
+        L = torch.empty((P, V, U, M), device=dev)
+        gI = torch.full((P, V, U), 1e-6, device=dev)
+        grads = [torch.zeros_like(v) for v in vols]
+        for _ in range(2):
+            pr.forward(vols, out={**out, "L": L})
+            pr.backward(L, gI, None, grads)
+        barrier_sync(ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_fa = max(1, min(args.steps, 3))
+        e0.record(stream)
+        for _ in range(n_fa):
+            pr.forward(vols, out={**out, "L": L})
+            pr.backward(L, gI, None, grads)
+        e1.record(stream)
+        barrier_sync(ws)
+        fa_ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
+        fa = {"value": ws * rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms}
+
+    # ---------------- CPU baseline (rank 0, N = 1) --------------------------
+    cpu = None
+    err = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        w._vols = vols
+        w._W = _weights_from_tables(w, local)
+        cpu, err = cpu_baseline(w, out["I"].cpu().numpy(), args.cpu_budget)
+
+    if rank == 0:
+        line = {
+            "metric": "rays/s (polyenergetic cone-beam forward projection)",
+            "value": value, "unit": "rays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded phantom per rank)",
+            "config": {"workload": w.name, "interp": args.interp, "volume": list(pr.shape_vol[::-1]), "materials": M,
+                       "views": P, "detector": [U, V], "energies": pr.E, "samples_per_ray": int(pr.info["intNum"]),
+                       "rays_per_step": rays, "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"independent objects x{ws}"},
+            "e2e": e2e,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "max_rel_err_vs_fp64_oracle": err,
+            "fwd_adjoint": fa,
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    pr.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _weights_from_tables(w, device):
+    """Energy weights W[e][v][u] in FP64 for the oracle, from the same device
+    tables the projector uses (grid, scintillator)."""
+    import torch
+
+    from ct_forward_projection_b200.projector import build_det_response, build_grid_table, scintillator_thickness
+    from oracle import oracle as O
+    g = w.geometry
+    U, V = int(g["dNumU"]), int(g["dNumV"])
+    E = len(w.energies)
+    G = None
+    if w.grid is not None:
+        ms, mi = w.grid_mu()
+        G = build_grid_table(g, w.grid, ms, mi, w.grid_layout, device=device).cpu().numpy()
+    D = None
+    if w.scint_mm is not None:
+        t = scintillator_thickness(U * V, w.scint_mm, w.scint_err_mm)
+        D = build_det_response(w.scint_mu(), torch.from_numpy(t).to(f"cuda:{device}"), 1.0).cpu().numpy()
+        D = D.reshape(E, V, U)
+    return O.energy_weights(g, w.spectrum(), G, w.grid_layout if G is not None else 0, D, w.I0Val)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,97 @@
+"""Builds the in-tree shared libraries with nvcc / g++ for sm_100a.
+
+  libctfp.so          the C-ABI projector (include/ctfp.h), CUDA kernels
+  libctfp_compat.so   the drop-in C++ classes over the C ABI
+  ctfp_forward_projection  the CLI (ForwardProjection::run equivalent)
+
+Run: python -m ct_forward_projection_b200.build
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+COMPAT = os.path.join(PKG, "compat")
+INCLUDE = os.path.join(ROOT, "include")
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+                     "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
+
+LIB = os.path.join(PKG, "libctfp.so")
+COMPAT_LIB = os.path.join(PKG, "libctfp_compat.so")
+CLI = os.path.join(PKG, "ctfp_forward_projection")
+
+CU_SOURCES = ["ctfp_api.cu", "ctfp_kernels.cu", "ctfp_batch.cu", "ctfp_tables.cu"]
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+
+
+def _deps(directory: str, exts: tuple[str, ...]) -> list[str]:
+    out = []
+    for d in (directory, INCLUDE):
+        for f in os.listdir(d):
+            if f.endswith(exts):
+                out.append(os.path.join(d, f))
+    return out
+
+
+def build_lib(force: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in CU_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    deps = _deps(CSRC, (".cu", ".cuh", ".h"))
+    if not force and _newer(LIB, deps):
+        return LIB
+    objdir = os.path.join(ROOT, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for s in srcs:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        _run([NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-dc", s, "-o", o])
+        objs.append(o)
+    _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    return LIB
+
+
+def build_compat(force: bool = False) -> str | None:
+    if not os.path.isdir(COMPAT):
+        return None
+    srcs = sorted(os.path.join(COMPAT, f) for f in os.listdir(COMPAT) if f.endswith(".cpp"))
+    if not srcs:
+        return None
+    deps = _deps(COMPAT, (".cpp", ".h")) + [LIB]
+    if not force and _newer(COMPAT_LIB, deps) and _newer(CLI, deps):
+        return COMPAT_LIB
+    lib_srcs = [s for s in srcs if not s.endswith("main.cpp")]
+    cflags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", INCLUDE, "-I", COMPAT]
+    _run(["g++", *cflags, "-shared", "-o", COMPAT_LIB, *lib_srcs, "-L", PKG, "-lctfp",
+          "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart"])
+    main = [s for s in srcs if s.endswith("main.cpp")]
+    if main:
+        _run(["g++", *cflags, "-o", CLI, *main, "-L", PKG, "-lctfp_compat", "-lctfp", "-Wl,-rpath,$ORIGIN",
+              "-L/usr/local/cuda/lib64", "-lcudart"])
+    return COMPAT_LIB
+
+
+def build(force: bool = False) -> None:
+    build_lib(force)
+    build_compat(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

@@ -1,0 +1,589 @@
+// ctfp_api.cu — the extern "C" boundary declared in include/ctfp.h.
+//
+// Ownership: the caller owns every buffer it passes (volumes, outputs,
+// checkpoints, gradients).  A plan owns its tables (view trigonometry, energy
+// weights W[E][V][U], flat field I0, attenuation table) and, in texture mode,
+// one cudaArray + texture object per material.  No call resets the device and
+// none exits: every failure is a ctfp_status plus a per-thread message.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ctfp.h"
+#include "ctfp_kernels.cuh"
+
+using namespace ctfp;
+
+struct ctfp_plan {
+    ctfp_geometry geom{};
+    ctfp_system_info info{};
+    int M = 0;
+    int interp = 0;
+    int device = 0;
+    GeomParams gp{};
+    double2* d_trig = nullptr;  // [P] (cos, sin) of the FP32 view angles
+    // spectral tables
+    int E = 0;
+    bool spectral_ready = false;
+    float* d_mu = nullptr;  // [E][M]
+    float* d_W = nullptr;   // [E][V][U]
+    float* d_I0 = nullptr;  // [V][U]
+    // texture mode
+    cudaArray_t arr[kMaxM] = {};
+    cudaTextureObject_t tex[kMaxM] = {};
+    LaunchShape shape{};
+    unsigned long long* d_count = nullptr;
+    // staging for ctfp_forward_host
+    float* h2d_vol[kMaxM] = {};
+    float* d2h_I = nullptr;
+    float* d2h_IAbs = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+ctfp_status fail(ctfp_status st, const std::string& msg)
+{
+    g_last_error = msg;
+    return st;
+}
+
+ctfp_status cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? CTFP_OOM : CTFP_CUDA_ERROR;
+}
+
+#define CTFP_CUDA(call)                                   \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Keeps the caller's current device and switches to the plan's for one call.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0) {
+            int cur = -1;
+            if (cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+        }
+    }
+};
+
+ctfp_status check_geometry(const ctfp_geometry* g)
+{
+    if (!g) return fail(CTFP_INVALID_ARG, "geometry is NULL");
+    if (g->pNumX <= 0 || g->pNumY <= 0 || g->pNumZ <= 0)
+        return fail(CTFP_INVALID_ARG, "pNumX/pNumY/pNumZ must be positive");
+    if ((double)g->pNumX * (double)g->pNumY * (double)g->pNumZ >= 2147483647.0)
+        return fail(CTFP_UNSUPPORTED, "volume must hold fewer than 2^31 voxels");
+    if (!(g->pLengthX > 0.f && g->pLengthY > 0.f && g->pLengthZ > 0.f))
+        return fail(CTFP_INVALID_ARG, "pLengthX/pLengthY/pLengthZ must be positive");
+    if (g->projNum <= 0 || g->projNum > 1000000) return fail(CTFP_INVALID_ARG, "projNum out of range");
+    if (g->dNumU <= 0 || g->dNumV <= 0 || g->dNumU > 65536 || g->dNumV > 65536)
+        return fail(CTFP_INVALID_ARG, "dNumU/dNumV out of range");
+    if (!(g->dSize > 0.f)) return fail(CTFP_INVALID_ARG, "dSize must be positive");
+    if (!(g->sod > 0.f) || !(g->sdd > g->sod)) return fail(CTFP_INVALID_ARG, "need 0 < sod < sdd");
+    if (g->rotatedDirection != 1 && g->rotatedDirection != -1)
+        return fail(CTFP_INVALID_ARG, "rotatedDirection must be +1 or -1");
+    if (g->reserved != 0) return fail(CTFP_INVALID_ARG, "reserved must be 0");
+    return CTFP_OK;
+}
+
+void compute_paras(const ctfp_geometry* g, ctfp_system_info* s)
+{
+    // CBCTForwardProj::computeParas (CBCTForwardProj.cpp:28-60), FP32 in the
+    // reference's order. Every product is stored through a volatile float
+    // before it is added, so no multiply-add contraction changes the result.
+    std::memset(s, 0, sizeof(*s));
+    volatile float t;
+    s->thetaStep = (float)360 / (float)g->projNum;
+    s->dHalfLU = (float)g->dNumU * g->dSize / 2;
+    s->dHalfLV = (float)g->dNumV * g->dSize / 2;
+    t = s->dHalfLU * s->dHalfLU;
+    volatile float t2 = g->sdd * g->sdd;
+    float rad = sqrtf(t + t2);
+    t = g->sod * s->dHalfLU;
+    s->FOVR = t / rad;
+    t = (g->sod - s->FOVR) * s->dHalfLV;
+    s->FOVH = t / g->sdd;
+    s->pSizeX = g->pLengthX / (float)g->pNumX;
+    s->pSizeY = g->pLengthY / (float)g->pNumY;
+    s->pSizeZ = g->pLengthZ / (float)g->pNumZ;
+    s->pHalfX = g->pLengthX / 2;
+    s->pHalfY = g->pLengthY / 2;
+    s->pHalfZ = g->pLengthZ / 2;
+    s->dx = (float)(0.5 * s->pSizeX);
+    s->dy = (float)(0.5 * s->pSizeY);
+    s->dz = (float)(0.5 * s->pSizeZ);
+    t = 2 * s->FOVR;
+    s->intNum = (int64_t)roundf(t / s->dx);
+}
+
+float view_angle(const ctfp_geometry* g, const ctfp_system_info* s, int64_t p)
+{
+    // CBCTPolyProjGPU.cu:51 with PI = acosf(-1) (CBCTPolyProjGPU.cuh:21). The
+    // reference's size_t product wraps for rotatedDirection = -1 and gives every
+    // view the same angle; the intended signed angle is used instead.
+    volatile float a = (float)p * s->thetaStep;
+    a = a / 180.0f;
+    a = a * acosf(-1.0f);
+    return g->rotatedDirection < 0 ? -a : a;
+}
+
+bool valid_interp(int i) { return i == INTERP_TRILINEAR || i == INTERP_TEXEMU || i == INTERP_TEXTURE; }
+
+ctfp_status make_textures(ctfp_plan* p)
+{
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaExtent ext = make_cudaExtent((size_t)p->geom.pNumX, (size_t)p->geom.pNumY, (size_t)p->geom.pNumZ);
+    for (int m = 0; m < p->M; m++) {
+        if (p->arr[m]) continue;
+        CTFP_CUDA(cudaMalloc3DArray(&p->arr[m], &cd, ext));
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = p->arr[m];
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        CTFP_CUDA(cudaCreateTextureObject(&p->tex[m], &rd, &td, nullptr));
+    }
+    return CTFP_OK;
+}
+
+void free_textures(ctfp_plan* p)
+{
+    for (int m = 0; m < kMaxM; m++) {
+        if (p->tex[m]) cudaDestroyTextureObject(p->tex[m]);
+        if (p->arr[m]) cudaFreeArray(p->arr[m]);
+        p->tex[m] = 0;
+        p->arr[m] = nullptr;
+    }
+}
+
+ctfp_status upload_textures(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
+{
+    for (int m = 0; m < p->M; m++) {
+        cudaMemcpy3DParms cp;
+        std::memset(&cp, 0, sizeof(cp));
+        cp.srcPtr = make_cudaPitchedPtr((void*)volumes[m], (size_t)p->geom.pNumX * sizeof(float),
+                                        (size_t)p->geom.pNumX, (size_t)p->geom.pNumY);
+        cp.dstArray = p->arr[m];
+        cp.extent = make_cudaExtent((size_t)p->geom.pNumX, (size_t)p->geom.pNumY, (size_t)p->geom.pNumZ);
+        cp.kind = cudaMemcpyDeviceToDevice;
+        CTFP_CUDA(cudaMemcpy3DAsync(&cp, st));
+    }
+    return CTFP_OK;
+}
+
+MarchParams base_params(const ctfp_plan* p)
+{
+    MarchParams prm;
+    std::memset(&prm, 0, sizeof(prm));
+    prm.g = p->gp;
+    prm.E = p->E;
+    prm.mu = p->d_mu;
+    prm.W = p->d_W;
+    prm.view0 = 0;
+    prm.n_views = (int)p->geom.projNum;
+    for (int m = 0; m < kMaxM; m++) prm.tex[m] = p->tex[m];
+    return prm;
+}
+
+ctfp_status check_volumes(const ctfp_plan* p, const float* const* volumes)
+{
+    if (!volumes) return fail(CTFP_INVALID_ARG, "volumes is NULL");
+    for (int m = 0; m < p->M; m++)
+        if (!volumes[m]) return fail(CTFP_INVALID_ARG, "volume pointer is NULL");
+    return CTFP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ctfp_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* ctfp_version(void) { return "ctfp 0.1.0 (sm_100a)"; }
+
+ctfp_status ctfp_compute_paras(const ctfp_geometry* g, ctfp_system_info* out)
+{
+    ctfp_status st = check_geometry(g);
+    if (st != CTFP_OK) return st;
+    if (!out) return fail(CTFP_INVALID_ARG, "out is NULL");
+    compute_paras(g, out);
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_view_angle(const ctfp_geometry* g, int64_t view, float* angle)
+{
+    ctfp_status st = check_geometry(g);
+    if (st != CTFP_OK) return st;
+    if (!angle || view < 0 || view >= g->projNum) return fail(CTFP_INVALID_ARG, "bad view or NULL angle");
+    ctfp_system_info s;
+    compute_paras(g, &s);
+    *angle = view_angle(g, &s, view);
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_t interp, int32_t device,
+                             ctfp_plan** out)
+{
+    if (!out) return fail(CTFP_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    ctfp_status st = check_geometry(g);
+    if (st != CTFP_OK) return st;
+    if (n_materials < 1 || n_materials > CTFP_MAX_MATERIALS)
+        return fail(CTFP_INVALID_ARG, "n_materials must be in [1, 4]");
+    if (!valid_interp(interp)) return fail(CTFP_INVALID_ARG, "unknown interp mode");
+    ctfp_system_info info;
+    compute_paras(g, &info);
+    if (info.intNum <= 0 || info.intNum > 100000000) return fail(CTFP_INVALID_ARG, "intNum out of range");
+    DeviceScope ds(device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    ctfp_plan* p = new (std::nothrow) ctfp_plan();
+    if (!p) return fail(CTFP_OOM, "host allocation failed");
+    p->geom = *g;
+    p->info = info;
+    p->M = n_materials;
+    p->interp = interp;
+    p->device = device;
+    GeomParams& gp = p->gp;
+    gp.nx = (int)g->pNumX; gp.ny = (int)g->pNumY; gp.nz = (int)g->pNumZ;
+    gp.U = (int)g->dNumU; gp.V = (int)g->dNumV; gp.P = (int)g->projNum;
+    gp.K = (int)info.intNum;
+    gp.dHalfLU = info.dHalfLU; gp.dHalfLV = info.dHalfLV; gp.dSize = g->dSize;
+    gp.sod = g->sod; gp.sdd = g->sdd; gp.FOVR = info.FOVR; gp.dx = info.dx;
+    gp.pHalfX = info.pHalfX; gp.pHalfY = info.pHalfY; gp.pHalfZ = info.pHalfZ;
+    gp.pSizeX = info.pSizeX; gp.pSizeY = info.pSizeY; gp.pSizeZ = info.pSizeZ;
+    std::vector<double2> trig((size_t)g->projNum);
+    for (int64_t k = 0; k < g->projNum; k++) {
+        const double a = (double)view_angle(g, &info, k);
+        trig[(size_t)k] = make_double2(std::cos(a), std::sin(a));
+    }
+    cudaError_t e = cudaMalloc(&p->d_trig, sizeof(double2) * trig.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_trig, trig.data(), sizeof(double2) * trig.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_count, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        ctfp_plan_destroy(p);
+        return cuda_fail(e, "plan allocation");
+    }
+    gp.trig = p->d_trig;
+    if (interp == INTERP_TEXTURE) {
+        st = make_textures(p);
+        if (st != CTFP_OK) {
+            std::string msg = g_last_error;
+            ctfp_plan_destroy(p);
+            return fail(st, msg);
+        }
+    }
+    *out = p;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_plan_destroy(ctfp_plan* p)
+{
+    if (!p) return CTFP_OK;
+    DeviceScope ds(p->device);
+    free_textures(p);
+    cudaFree(p->d_trig);
+    cudaFree(p->d_mu);
+    cudaFree(p->d_W);
+    cudaFree(p->d_I0);
+    cudaFree(p->d_count);
+    for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
+    cudaFree(p->d2h_I);
+    cudaFree(p->d2h_IAbs);
+    delete p;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_plan_get_system_info(const ctfp_plan* p, ctfp_system_info* out)
+{
+    if (!p || !out) return fail(CTFP_INVALID_ARG, "NULL argument");
+    *out = p->info;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_plan_set_interp(ctfp_plan* p, int32_t interp)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    if (!valid_interp(interp)) return fail(CTFP_INVALID_ARG, "unknown interp mode");
+    DeviceScope ds(p->device);
+    if (interp == INTERP_TEXTURE) {
+        ctfp_status st = make_textures(p);
+        if (st != CTFP_OK) return st;
+    }
+    p->interp = interp;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_set_spectral_tables(ctfp_plan* p, int32_t E, const float* spectrum, const float* mu,
+                                     const float* grid, int32_t grid_layout, const float* det_response, float I0Val)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    if (E < 1 || E > CTFP_MAX_ENERGIES) return fail(CTFP_INVALID_ARG, "n_energies must be in [1, 256]");
+    if (!spectrum || !mu) return fail(CTFP_INVALID_ARG, "spectrum and mu are required");
+    if (grid_layout < 0 || grid_layout > 2) return fail(CTFP_INVALID_ARG, "unknown grid layout");
+    if (grid_layout != 0 && !grid) return fail(CTFP_INVALID_ARG, "grid table is NULL");
+    if (!(I0Val >= 0.f)) return fail(CTFP_INVALID_ARG, "I0Val must be non-negative");
+    DeviceScope ds(p->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    const int64_t U = p->geom.dNumU, V = p->geom.dNumV, npix = U * V;
+    const size_t nG = grid_layout == 1 ? (size_t)E * U : grid_layout == 2 ? (size_t)E * npix : 0;
+    const size_t nD = det_response ? (size_t)E * npix : 0;
+    float *dS = nullptr, *dG = nullptr, *dD = nullptr;
+    cudaFree(p->d_mu); p->d_mu = nullptr;
+    cudaFree(p->d_W); p->d_W = nullptr;
+    cudaFree(p->d_I0); p->d_I0 = nullptr;
+    p->spectral_ready = false;
+    cudaError_t e = cudaMalloc(&p->d_mu, sizeof(float) * (size_t)E * p->M);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_W, sizeof(float) * (size_t)E * npix);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_I0, sizeof(float) * (size_t)npix);
+    if (e == cudaSuccess) e = cudaMalloc(&dS, sizeof(float) * (size_t)E);
+    if (e == cudaSuccess && nG) e = cudaMalloc(&dG, sizeof(float) * nG);
+    if (e == cudaSuccess && nD) e = cudaMalloc(&dD, sizeof(float) * nD);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_mu, mu, sizeof(float) * (size_t)E * p->M, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dS, spectrum, sizeof(float) * (size_t)E, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nG) e = cudaMemcpy(dG, grid, sizeof(float) * nG, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nD) e = cudaMemcpy(dD, det_response, sizeof(float) * nD, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_weights(dS, dG, grid_layout, dD, I0Val, E, (int)U, (int)V, p->d_W, p->d_I0, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(dS);
+    cudaFree(dG);
+    cudaFree(dD);
+    if (e != cudaSuccess) return cuda_fail(e, "ctfp_set_spectral_tables");
+    p->E = E;
+    p->spectral_ready = true;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float* L, void* stream)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    ctfp_status st = check_volumes(p, volumes);
+    if (st != CTFP_OK) return st;
+    if (!L) return fail(CTFP_INVALID_ARG, "L is NULL");
+    DeviceScope ds(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MarchParams prm = base_params(p);
+    for (int m = 0; m < p->M; m++) prm.vol[m] = volumes[m];
+    prm.L = L;
+    if (p->interp == INTERP_TEXTURE) {
+        st = upload_textures(p, volumes, s);
+        if (st != CTFP_OK) return st;
+    }
+    CTFP_CUDA(launch_forward(prm, p->M, p->interp, false, p->shape, s));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_forward(ctfp_plan* p, const float* const* volumes, float* I, float* IAbsorb, float* I0,
+                         float* L_ckpt, void* stream)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    ctfp_status st = check_volumes(p, volumes);
+    if (st != CTFP_OK) return st;
+    if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    DeviceScope ds(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MarchParams prm = base_params(p);
+    for (int m = 0; m < p->M; m++) prm.vol[m] = volumes[m];
+    prm.I = I;
+    prm.IAbs = IAbsorb;
+    prm.L = L_ckpt;
+    if (p->interp == INTERP_TEXTURE) {
+        st = upload_textures(p, volumes, s);
+        if (st != CTFP_OK) return st;
+    }
+    CTFP_CUDA(launch_forward(prm, p->M, p->interp, true, p->shape, s));
+    if (I0)
+        CTFP_CUDA(cudaMemcpyAsync(I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
+                                  cudaMemcpyDeviceToDevice, s));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_forward_host(ctfp_plan* p, const float* const* host_volumes, float* host_I, float* host_IAbsorb,
+                              float* host_I0, void* stream)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    ctfp_status st = check_volumes(p, host_volumes);
+    if (st != CTFP_OK) return st;
+    if (!host_I || !host_IAbsorb) return fail(CTFP_INVALID_ARG, "host_I and host_IAbsorb are required");
+    if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    DeviceScope ds(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nvox = (size_t)p->geom.pNumX * p->geom.pNumY * p->geom.pNumZ;
+    const size_t nray = (size_t)p->geom.projNum * p->geom.dNumU * p->geom.dNumV;
+    for (int m = 0; m < p->M; m++)
+        if (!p->h2d_vol[m]) CTFP_CUDA(cudaMalloc(&p->h2d_vol[m], nvox * sizeof(float)));
+    if (!p->d2h_I) CTFP_CUDA(cudaMalloc(&p->d2h_I, nray * sizeof(float)));
+    if (!p->d2h_IAbs) CTFP_CUDA(cudaMalloc(&p->d2h_IAbs, nray * sizeof(float)));
+    const float* dv[kMaxM] = {};
+    for (int m = 0; m < p->M; m++) {
+        CTFP_CUDA(cudaMemcpyAsync(p->h2d_vol[m], host_volumes[m], nvox * sizeof(float), cudaMemcpyHostToDevice, s));
+        dv[m] = p->h2d_vol[m];
+    }
+    st = ctfp_forward(p, dv, p->d2h_I, p->d2h_IAbs, nullptr, nullptr, stream);
+    if (st != CTFP_OK) return st;
+    CTFP_CUDA(cudaMemcpyAsync(host_I, p->d2h_I, nray * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CTFP_CUDA(cudaMemcpyAsync(host_IAbsorb, p->d2h_IAbs, nray * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (host_I0)
+        CTFP_CUDA(cudaMemcpyAsync(host_I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
+                                  cudaMemcpyDeviceToHost, s));
+    CTFP_CUDA(cudaStreamSynchronize(s));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_spectral_from_L(ctfp_plan* p, const float* L, float* I, float* IAbsorb, void* stream)
+{
+    if (!p || !L) return fail(CTFP_INVALID_ARG, "NULL argument");
+    if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    DeviceScope ds(p->device);
+    MarchParams prm = base_params(p);
+    prm.Lin = L;
+    prm.I = I;
+    prm.IAbs = IAbsorb;
+    CTFP_CUDA(launch_spectral_from_L(prm, p->M, (cudaStream_t)stream));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_finalize_counts(int64_t n_pix, int64_t n_views, const float* I, const float* IAbsorb,
+                                 const float* I0, uint32_t* Ipoly, uint32_t* IAbsPoly, float* proj, void* stream)
+{
+    if (n_pix < 0 || n_views < 0) return fail(CTFP_INVALID_ARG, "negative size");
+    if (proj && (!I0 || !I)) return fail(CTFP_INVALID_ARG, "proj needs I and I0");
+    CTFP_CUDA(launch_finalize(n_pix, n_views, I, IAbsorb, I0, Ipoly, IAbsPoly, proj, (cudaStream_t)stream));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_backward(ctfp_plan* p, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                          float* const* g_volumes, void* stream)
+{
+    if (!p || !L_ckpt || !g_volumes) return fail(CTFP_INVALID_ARG, "NULL argument");
+    if (!gI && !gIAbsorb) return fail(CTFP_INVALID_ARG, "need gI or gIAbsorb");
+    if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    for (int m = 0; m < p->M; m++)
+        if (!g_volumes[m]) return fail(CTFP_INVALID_ARG, "gradient volume pointer is NULL");
+    DeviceScope ds(p->device);
+    MarchParams prm = base_params(p);
+    prm.Lin = L_ckpt;
+    prm.gI = gI;
+    prm.gIAbs = gIAbsorb;
+    for (int m = 0; m < p->M; m++) prm.gvol[m] = g_volumes[m];
+    CTFP_CUDA(launch_backward(prm, p->M, p->interp, false, p->shape, (cudaStream_t)stream));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* p, const float* gL, float* const* g_volumes, void* stream)
+{
+    if (!p || !gL || !g_volumes) return fail(CTFP_INVALID_ARG, "NULL argument");
+    for (int m = 0; m < p->M; m++)
+        if (!g_volumes[m]) return fail(CTFP_INVALID_ARG, "gradient volume pointer is NULL");
+    DeviceScope ds(p->device);
+    MarchParams prm = base_params(p);
+    prm.Lin = gL;
+    for (int m = 0; m < p->M; m++) prm.gvol[m] = g_volumes[m];
+    CTFP_CUDA(launch_backward(prm, p->M, p->interp, true, p->shape, (cudaStream_t)stream));
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_sample_volume(const float* volume, int64_t nx, int64_t ny, int64_t nz, int32_t interp,
+                               const float* points, int64_t n, float* out, void* stream)
+{
+    if (!volume || !points || !out || n < 0) return fail(CTFP_INVALID_ARG, "bad argument");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || (double)nx * ny * nz >= 2147483647.0)
+        return fail(CTFP_INVALID_ARG, "bad volume size");
+    if (!valid_interp(interp)) return fail(CTFP_INVALID_ARG, "unknown interp mode");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    if (interp == INTERP_TEXTURE) {
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+        cudaExtent ext = make_cudaExtent((size_t)nx, (size_t)ny, (size_t)nz);
+        CTFP_CUDA(cudaMalloc3DArray(&arr, &cd, ext));
+        cudaMemcpy3DParms cp;
+        std::memset(&cp, 0, sizeof(cp));
+        cp.srcPtr = make_cudaPitchedPtr((void*)volume, (size_t)nx * sizeof(float), (size_t)nx, (size_t)ny);
+        cp.dstArray = arr;
+        cp.extent = ext;
+        cp.kind = cudaMemcpyDeviceToDevice;
+        cudaError_t e = cudaMemcpy3DAsync(&cp, s);
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        if (e == cudaSuccess) e = cudaCreateTextureObject(&tex, &rd, &td, nullptr);
+        if (e != cudaSuccess) {
+            cudaFreeArray(arr);
+            return cuda_fail(e, "texture setup");
+        }
+    }
+    cudaError_t e = launch_sample_points(volume, tex, (int)nx, (int)ny, (int)nz, interp, points, n, out, s);
+    if (interp == INTERP_TEXTURE) {
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = e2;
+        cudaDestroyTextureObject(tex);
+        cudaFreeArray(arr);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "ctfp_sample_volume");
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_count_support_samples(ctfp_plan* p, int64_t* out)
+{
+    if (!p || !out) return fail(CTFP_INVALID_ARG, "NULL argument");
+    DeviceScope ds(p->device);
+    CTFP_CUDA(cudaMemset(p->d_count, 0, sizeof(unsigned long long)));
+    CTFP_CUDA(launch_count_support(p->gp, p->d_count, 0));
+    unsigned long long h = 0;
+    CTFP_CUDA(cudaMemcpy(&h, p->d_count, sizeof(h), cudaMemcpyDeviceToHost));
+    *out = (int64_t)h;
+    return CTFP_OK;
+}
+
+}  // extern "C"
+
+// Internal accessors for the other translation units.
+namespace ctfp {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const GeomParams& plan_geom(const ctfp_plan* p) { return p->gp; }
+int plan_materials(const ctfp_plan* p) { return p->M; }
+int plan_interp(const ctfp_plan* p) { return p->interp; }
+int plan_device(const ctfp_plan* p) { return p->device; }
+int plan_energies(const ctfp_plan* p) { return p->spectral_ready ? p->E : 0; }
+const float* plan_mu(const ctfp_plan* p) { return p->d_mu; }
+const float* plan_W(const ctfp_plan* p) { return p->d_W; }
+LaunchShape& plan_shape(ctfp_plan* p) { return p->shape; }
+}  // namespace ctfp
+
+extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, int32_t tile_v, int32_t views_per_cta)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    if (tile_u < 1 || tile_v < 1 || tile_u * tile_v > 256 || (tile_u * tile_v) % 32 != 0 || views_per_cta < 1)
+        return fail(CTFP_INVALID_ARG, "tile_u*tile_v must be a multiple of 32 and at most 256");
+    p->shape.tile_u = tile_u;
+    p->shape.tile_v = tile_v;
+    p->shape.views_per_cta = views_per_cta;
+    return CTFP_OK;
+}

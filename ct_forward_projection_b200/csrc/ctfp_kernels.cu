@@ -1,0 +1,435 @@
+// ctfp_kernels.cu — the march kernels (K1 ray march fused with the K2
+// spectral epilogue), the adjoint scatter, and small helper kernels.
+//
+// K1+K2 replaces, for every (view, pixel) ray, the reference's
+//   transformKernel (CBCTPolyProjGPU.cu:1902-1924)  K*U*V samples to HBM per view
+//   forward*Kernel  (CBCTPolyProjGPU.cu:1980-2169)  per-ray sum + Beer-Lambert per energy
+//   host energy loop (CBCTPolyForwardProjGrid.cpp:159-177, CBCTForwardProj.cpp:65-76)
+// with one pass: samples stay in registers, each material is marched once for
+// all energies (sum_m mu[e][m] * L_m equals the reference's per-energy
+// mu_E-volume integral because trilinear interpolation is linear in the voxel
+// values), and the energy sum runs on the device in compensated FP32.
+#include "ctfp_kernels.cuh"
+
+namespace ctfp {
+
+namespace {
+
+template <int M, int MODE>
+__device__ __forceinline__ void sample_point(const MarchParams& prm, double cx, double cy, double cz, float* val)
+{
+    if (MODE == INTERP_TEXTURE) {
+        // the reference's own fetch: tex3D(c + 0.5) on a border/linear texture
+        const float tx = (float)(cx + 0.5), ty = (float)(cy + 0.5), tz = (float)(cz + 0.5);
+#pragma unroll
+        for (int m = 0; m < M; m++) val[m] = tex3D<float>(prm.tex[m], tx, ty, tz);
+    } else {
+        const Corner c = corner_of<MODE>(cx, cy, cz);
+        gather_interp<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, val);
+    }
+}
+
+// L_m for one ray, compensated FP32 sum times dx.
+template <int M, int MODE>
+__device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, int u, float* L)
+{
+    const RaySeg s = ray_segment(prm.g, p, v, u);
+    float acc[M], cmp[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+#pragma unroll 2
+    for (int i = s.i0; i < s.i1; i++) {
+        const double t = (double)i;
+        float val[M];
+        sample_point<M, MODE>(prm, fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az), val);
+#pragma unroll
+        for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
+}
+
+// exp(-a) and 1 - exp(-a), each to a few ulp relative, with one transcendental.
+__device__ __forceinline__ void transmit(float a, float& ex, float& om)
+{
+    if (a < 0.25f) {
+        om = -expm1f(-a);
+        ex = 1.0f - om;
+    } else {
+        ex = expf(-a);
+        om = 1.0f - ex;
+    }
+}
+
+// K2: I = sum_e W_e exp(-sum_m mu_em L_m), IAbs = sum_e W_e (1 - exp(...)).
+template <int M>
+__device__ __forceinline__ void spectral(const float* s_mu, int E, const float* __restrict__ W, int64_t pix,
+                                         int64_t npix, const float* L, float& I, float& IAbs)
+{
+    float sI = 0.f, cI = 0.f, sA = 0.f, cA = 0.f;
+    for (int e = 0; e < E; e++) {
+        float att = 0.f;
+#pragma unroll
+        for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
+        const float w = __ldg(W + (int64_t)e * npix + pix);
+        float ex, om;
+        transmit(att, ex, om);
+        kahan_add(sI, cI, w * ex);
+        kahan_add(sA, cA, w * om);
+    }
+    I = sI - cI;
+    IAbs = sA - cA;
+}
+
+__device__ __forceinline__ void load_mu(float* s_mu, const float* mu, int n)
+{
+    const int nt = blockDim.x * blockDim.y;
+    for (int k = threadIdx.y * blockDim.x + threadIdx.x; k < n; k += nt) s_mu[k] = mu[k];
+    __syncthreads();
+}
+
+template <int M>
+__device__ __forceinline__ void store_L(float* L, int64_t ray, const float* l)
+{
+    float* q = L + ray * M;
+    if (M == 4) {
+        *reinterpret_cast<float4*>(q) = make_float4(l[0], l[1], l[2], l[3]);
+    } else if (M == 2) {
+        *reinterpret_cast<float2*>(q) = make_float2(l[0], l[1]);
+    } else {
+#pragma unroll
+        for (int m = 0; m < M; m++) q[m] = l[m];
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void load_L(const float* L, int64_t ray, float* l)
+{
+    const float* q = L + ray * M;
+    if (M == 4) {
+        const float4 a = *reinterpret_cast<const float4*>(q);
+        l[0] = a.x; l[1] = a.y; l[2] = a.z; l[3] = a.w;
+    } else if (M == 2) {
+        const float2 a = *reinterpret_cast<const float2*>(q);
+        l[0] = a.x; l[1] = a.y;
+    } else {
+#pragma unroll
+        for (int m = 0; m < M; m++) l[m] = q[m];
+    }
+}
+
+// K1+K2. Grid: x = pixel tiles along u, y = along v, z = view groups.
+template <int M, int MODE, bool SPECTRAL>
+__global__ void __launch_bounds__(256) k_forward(const MarchParams prm)
+{
+    extern __shared__ float s_mu[];
+    if (SPECTRAL) load_mu(s_mu, prm.mu, prm.E * M);
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    if (u >= prm.g.U || v >= prm.g.V) return;
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t pix = (int64_t)v * prm.g.U + u;
+    const int pend = prm.view0 + prm.n_views;
+    for (int k = 0; k < prm.views_per_cta; k++) {
+        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        if (p >= pend) break;
+        float L[M];
+        march_ray<M, MODE>(prm, p, v, u, L);
+        const int64_t ray = (int64_t)p * npix + pix;
+        if (prm.L) store_L<M>(prm.L, ray, L);
+        if (SPECTRAL) {
+            float I, A;
+            spectral<M>(s_mu, prm.E, prm.W, pix, npix, L, I, A);
+            if (prm.I) prm.I[ray] = I;
+            if (prm.IAbs) prm.IAbs[ray] = A;
+        }
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) k_spectral_from_L(const MarchParams prm)
+{
+    extern __shared__ float s_mu[];
+    load_mu(s_mu, prm.mu, prm.E * M);
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t nray = npix * prm.g.P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * blockDim.y;
+    for (int64_t ray = (int64_t)blockIdx.x * blockDim.x * blockDim.y + threadIdx.y * blockDim.x + threadIdx.x;
+         ray < nray; ray += stride) {
+        float L[M];
+        load_L<M>(prm.Lin, ray, L);
+        float I, A;
+        spectral<M>(s_mu, prm.E, prm.W, ray % npix, npix, L, I, A);
+        if (prm.I) prm.I[ray] = I;
+        if (prm.IAbs) prm.IAbs[ray] = A;
+    }
+}
+
+// Adjoint: spectral-weight recompute from the checkpoint, then the matched
+// ray march scattering the transposed trilinear weights with FP32 atomics.
+// FROM_GL: the input is dLoss/dL directly (transpose of the line integrals).
+template <int M, int MODE, bool FROM_GL>
+__global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
+{
+    extern __shared__ float s_mu[];
+    if (!FROM_GL) load_mu(s_mu, prm.mu, prm.E * M);
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    if (u >= prm.g.U || v >= prm.g.V) return;
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t pix = (int64_t)v * prm.g.U + u;
+    const int pend = prm.view0 + prm.n_views;
+    for (int k = 0; k < prm.views_per_cta; k++) {
+        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        if (p >= pend) break;
+        const int64_t ray = (int64_t)p * npix + pix;
+        float g[M];
+        if (FROM_GL) {
+            load_L<M>(prm.Lin, ray, g);
+#pragma unroll
+            for (int m = 0; m < M; m++) g[m] *= prm.g.dx;
+        } else {
+            float L[M], S[M];
+            load_L<M>(prm.Lin, ray, L);
+#pragma unroll
+            for (int m = 0; m < M; m++) S[m] = 0.f;
+            for (int e = 0; e < prm.E; e++) {
+                float att = 0.f;
+#pragma unroll
+                for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
+                const float Ie = __ldg(prm.W + (int64_t)e * npix + pix) * expf(-att);
+#pragma unroll
+                for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
+            }
+            const float gd = ((prm.gIAbs ? prm.gIAbs[ray] : 0.f) - (prm.gI ? prm.gI[ray] : 0.f)) * prm.g.dx;
+#pragma unroll
+            for (int m = 0; m < M; m++) g[m] = gd * S[m];
+        }
+        bool any = false;
+#pragma unroll
+        for (int m = 0; m < M; m++) any |= (g[m] != 0.f);
+        if (!any) continue;
+        const RaySeg s = ray_segment(prm.g, p, v, u);
+        for (int i = s.i0; i < s.i1; i++) {
+            const double t = (double)i;
+            const Corner c = corner_of<MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(
+                fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+            scatter_interp<M>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
+        }
+    }
+}
+
+// W[e][k] = ((I0Val * S_e) * G_e) * D_e in the reference's multiplication order
+// (CBCTPolyProjGPU.cu:1994); I0[k] = compensated sum over e
+// (CBCTPolyForwardProjGrid.cpp:330-339).
+__global__ void k_weights(const float* __restrict__ S, const float* __restrict__ G, int grid_layout,
+                          const float* __restrict__ D, float I0Val, int E, int U, int V, float* W, float* I0)
+{
+    const int64_t npix = (int64_t)U * V;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < npix; k += (int64_t)gridDim.x * blockDim.x) {
+        const int u = (int)(k % U);
+        float s = 0.f, c = 0.f;
+        for (int e = 0; e < E; e++) {
+            float w = I0Val * S[e];
+            if (grid_layout == 1) w = w * G[(int64_t)e * U + u];
+            if (grid_layout == 2) w = w * G[(int64_t)e * npix + k];
+            if (D) w = w * D[(int64_t)e * npix + k];
+            W[(int64_t)e * npix + k] = w;
+            kahan_add(s, c, w);
+        }
+        I0[k] = s - c;
+    }
+}
+
+// Ipoly = (uint32)floorf(I); proj = logf(I0 / Ipoly) (CBCTForwardProj.cpp:79-90, 376-387).
+__global__ void k_finalize(int64_t n_pix, int64_t n, const float* __restrict__ I, const float* __restrict__ IAbs,
+                           const float* __restrict__ I0, uint32_t* Ipoly, uint32_t* IAbsPoly, float* proj)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        if (I) {
+            const uint32_t ip = (uint32_t)floorf(I[k]);
+            if (Ipoly) Ipoly[k] = ip;
+            if (proj && I0) proj[k] = logf(I0[k % n_pix] / (float)ip);
+        }
+        if (IAbs && IAbsPoly) IAbsPoly[k] = (uint32_t)floorf(IAbs[k]);
+    }
+}
+
+__global__ void k_sample_points(const float* vol, cudaTextureObject_t tex, int nx, int ny, int nz, int interp,
+                                const float* pts, int64_t n, float* out)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double cx = pts[3 * k], cy = pts[3 * k + 1], cz = pts[3 * k + 2];
+        float val;
+        if (interp == INTERP_TEXTURE) {
+            val = tex3D<float>(tex, (float)(cx + 0.5), (float)(cy + 0.5), (float)(cz + 0.5));
+        } else {
+            const float* vp[1] = {vol};
+            const Corner c = interp == INTERP_TEXEMU ? corner_of<INTERP_TEXEMU>(cx, cy, cz)
+                                                     : corner_of<INTERP_TRILINEAR>(cx, cy, cz);
+            gather_interp<1>(vp, nx, ny, nz, c, &val);
+        }
+        out[k] = val;
+    }
+}
+
+// Exact count of samples whose trilinear footprint touches the volume.
+__global__ void k_count_support(const GeomParams g, unsigned long long* out)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    unsigned long long n = 0;
+    if (u < g.U && v < g.V) {
+        for (int p = blockIdx.z; p < g.P; p += gridDim.z) {
+            const RaySeg s = ray_segment(g, p, v, u);
+            for (int i = s.i0; i < s.i1; i++) {
+                const double t = (double)i;
+                const double cx = fma(t, s.bx, s.ax), cy = fma(t, s.by, s.ay), cz = fma(t, s.bz, s.az);
+                n += (cx > -1.0 && cy > -1.0 && cz > -1.0 && cx < (double)g.nx && cy < (double)g.ny &&
+                      cz < (double)g.nz);
+            }
+        }
+    }
+    // warp reduce then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, n);
+}
+
+template <int M, int MODE>
+cudaError_t fwd_dispatch_spec(const MarchParams& prm, bool spec, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+{
+    if (spec) k_forward<M, MODE, true><<<grid, block, smem, st>>>(prm);
+    else k_forward<M, MODE, false><<<grid, block, 0, st>>>(prm);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, bool spec, dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st)
+{
+    switch (interp) {
+        case INTERP_TRILINEAR: return fwd_dispatch_spec<M, INTERP_TRILINEAR>(prm, spec, grid, block, smem, st);
+        case INTERP_TEXEMU: return fwd_dispatch_spec<M, INTERP_TEXEMU>(prm, spec, grid, block, smem, st);
+        case INTERP_TEXTURE: return fwd_dispatch_spec<M, INTERP_TEXTURE>(prm, spec, grid, block, smem, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int M>
+cudaError_t bwd_dispatch(const MarchParams& prm, int interp, bool from_gL, dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t st)
+{
+    const bool tri = interp == INTERP_TRILINEAR;
+    if (from_gL) {
+        if (tri) k_backward<M, INTERP_TRILINEAR, true><<<grid, block, 0, st>>>(prm);
+        else k_backward<M, INTERP_TEXEMU, true><<<grid, block, 0, st>>>(prm);
+    } else {
+        if (tri) k_backward<M, INTERP_TRILINEAR, false><<<grid, block, smem, st>>>(prm);
+        else k_backward<M, INTERP_TEXEMU, false><<<grid, block, smem, st>>>(prm);
+    }
+    return cudaGetLastError();
+}
+
+dim3 march_grid(const MarchParams& prm, const LaunchShape& ls)
+{
+    return dim3((prm.g.U + ls.tile_u - 1) / ls.tile_u, (prm.g.V + ls.tile_v - 1) / ls.tile_v,
+                (prm.n_views + ls.views_per_cta - 1) / ls.views_per_cta);
+}
+
+}  // namespace
+
+cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, bool do_spectral, const LaunchShape& ls,
+                           cudaStream_t st)
+{
+    MarchParams prm = prm_in;
+    prm.views_per_cta = ls.views_per_cta;
+    const dim3 block(ls.tile_u, ls.tile_v), grid = march_grid(prm, ls);
+    const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
+    switch (M) {
+        case 1: return fwd_dispatch_mode<1>(prm, interp, do_spectral, grid, block, smem, st);
+        case 2: return fwd_dispatch_mode<2>(prm, interp, do_spectral, grid, block, smem, st);
+        case 3: return fwd_dispatch_mode<3>(prm, interp, do_spectral, grid, block, smem, st);
+        case 4: return fwd_dispatch_mode<4>(prm, interp, do_spectral, grid, block, smem, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st)
+{
+    const dim3 block(256, 1);
+    const int64_t nray = (int64_t)prm.g.U * prm.g.V * prm.g.P;
+    int64_t nb = (nray + 255) / 256;
+    if (nb > 148 * 64) nb = 148 * 64;
+    if (nb == 0) return cudaSuccess;
+    const size_t smem = sizeof(float) * (size_t)prm.E * M;
+    switch (M) {
+        case 1: k_spectral_from_L<1><<<(unsigned)nb, block, smem, st>>>(prm); break;
+        case 2: k_spectral_from_L<2><<<(unsigned)nb, block, smem, st>>>(prm); break;
+        case 3: k_spectral_from_L<3><<<(unsigned)nb, block, smem, st>>>(prm); break;
+        case 4: k_spectral_from_L<4><<<(unsigned)nb, block, smem, st>>>(prm); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backward(const MarchParams& prm_in, int M, int interp, bool from_gL, const LaunchShape& ls,
+                            cudaStream_t st)
+{
+    MarchParams prm = prm_in;
+    prm.views_per_cta = ls.views_per_cta;
+    const dim3 block(ls.tile_u, ls.tile_v), grid = march_grid(prm, ls);
+    const size_t smem = sizeof(float) * (size_t)prm.E * M;
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
+    switch (M) {
+        case 1: return bwd_dispatch<1>(prm, interp, from_gL, grid, block, smem, st);
+        case 2: return bwd_dispatch<2>(prm, interp, from_gL, grid, block, smem, st);
+        case 3: return bwd_dispatch<3>(prm, interp, from_gL, grid, block, smem, st);
+        case 4: return bwd_dispatch<4>(prm, interp, from_gL, grid, block, smem, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_weights(const float* spectrum, const float* grid, int grid_layout, const float* det, float I0Val,
+                           int E, int U, int V, float* W, float* I0, cudaStream_t st)
+{
+    const int64_t npix = (int64_t)U * V;
+    int64_t nb = (npix + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    if (nb == 0) return cudaSuccess;
+    k_weights<<<(unsigned)nb, 256, 0, st>>>(spectrum, grid, grid_layout, det, I0Val, E, U, V, W, I0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(int64_t n_pix, int64_t n_views, const float* I, const float* IAbs, const float* I0,
+                            uint32_t* Ipoly, uint32_t* IAbsPoly, float* proj, cudaStream_t st)
+{
+    const int64_t n = n_pix * n_views;
+    int64_t nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    if (nb == 0) return cudaSuccess;
+    k_finalize<<<(unsigned)nb, 256, 0, st>>>(n_pix, n, I, IAbs, I0, Ipoly, IAbsPoly, proj);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample_points(const float* vol, cudaTextureObject_t tex, int nx, int ny, int nz, int interp,
+                                 const float* pts, int64_t n, float* out, cudaStream_t st)
+{
+    int64_t nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    if (nb == 0) return cudaSuccess;
+    k_sample_points<<<(unsigned)nb, 256, 0, st>>>(vol, tex, nx, ny, nz, interp, pts, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, cudaStream_t st)
+{
+    const dim3 block(32, 8);
+    int gz = g.P < 64 ? g.P : 64;
+    const dim3 grid((g.U + 31) / 32, (g.V + 7) / 8, gz > 0 ? gz : 1);
+    if (g.P == 0 || g.U == 0 || g.V == 0) return cudaSuccess;
+    k_count_support<<<grid, block, 0, st>>>(g, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ctfp

@@ -1,0 +1,46 @@
+// ctfp_kernels.cuh — kernel parameter blocks and launcher declarations.
+#pragma once
+
+#include "ctfp_device.cuh"
+
+namespace ctfp {
+
+// One problem as the march kernels see it.
+struct MarchParams {
+    GeomParams g;
+    const float* vol[kMaxM];          // material densities [nz][ny][nx]
+    cudaTextureObject_t tex[kMaxM];   // same volumes as textures (TEXTURE mode)
+    float* L;                         // [P][V][U][M] path integrals (out, may be null)
+    const float* Lin;                 // [P][V][U][M] path integrals (in, epilogue/adjoint)
+    float* I;                         // [P][V][U] (may be null)
+    float* IAbs;                      // [P][V][U] (may be null)
+    const float* W;                   // [E][V][U] energy weights I0Val*S*G*D
+    const float* mu;                  // [E][M] attenuation per density, 1/mm per g/cm^3
+    const float* gI;                  // [P][V][U] dLoss/dI (adjoint)
+    const float* gIAbs;               // [P][V][U] dLoss/dIAbsorb (adjoint, may be null)
+    float* gvol[kMaxM];               // gradient volumes (adjoint)
+    int E;
+    int view0;                        // first view of this launch
+    int n_views;                      // views in this launch
+    int views_per_cta;                // views each CTA marches for its pixel tile
+};
+
+struct LaunchShape {
+    int tile_u = 32, tile_v = 8, views_per_cta = 1;
+};
+
+// Launchers; all return cudaGetLastError() of the launch.
+cudaError_t launch_forward(const MarchParams& prm, int M, int interp, bool do_spectral, const LaunchShape& ls,
+                           cudaStream_t st);
+cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st);
+cudaError_t launch_backward(const MarchParams& prm, int M, int interp, bool from_gL, const LaunchShape& ls,
+                            cudaStream_t st);
+cudaError_t launch_weights(const float* spectrum, const float* grid, int grid_layout, const float* det,
+                           float I0Val, int E, int U, int V, float* W, float* I0, cudaStream_t st);
+cudaError_t launch_finalize(int64_t n_pix, int64_t n_views, const float* I, const float* IAbs, const float* I0,
+                            uint32_t* Ipoly, uint32_t* IAbsPoly, float* proj, cudaStream_t st);
+cudaError_t launch_sample_points(const float* vol, cudaTextureObject_t tex, int nx, int ny, int nz, int interp,
+                                 const float* pts, int64_t n, float* out, cudaStream_t st);
+cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, cudaStream_t st);
+
+}  // namespace ctfp

@@ -1,0 +1,292 @@
+"""Python host mirror of the projector over the C ABI (include/ctfp.h).
+
+`Projector` is one plan: the geometry of CTScanParas (DataType.h:33-55), the
+number of materials, the sampler, and the spectral tables.  Device memory is
+torch tensors on the plan's CUDA device; every compute call goes through
+libctfp.so, and there is no other compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import Geometry, GridParams, SystemInfo, call, lib, ptr_array
+
+INTERP = {"trilinear": capi.INTERP_TRILINEAR, "texemu": capi.INTERP_TEXEMU, "texture": capi.INTERP_TEXTURE}
+
+
+def make_geometry(d: dict) -> Geometry:
+    g = Geometry()
+    for k in ("pNumX", "pNumY", "pNumZ", "projNum", "dNumU", "dNumV"):
+        setattr(g, k, int(d[k]))
+    for k in ("pLengthX", "pLengthY", "pLengthZ", "dSize", "sod", "sdd"):
+        setattr(g, k, float(d[k]))
+    g.rotatedDirection = int(d.get("rotatedDirection", 1))
+    g.reserved = 0
+    return g
+
+
+def compute_paras(geom: dict) -> dict:
+    """CBCTForwardProj::computeParas (CBCTForwardProj.cpp:23-62) via the library."""
+    info = SystemInfo()
+    call("ctfp_compute_paras", C.byref(make_geometry(geom)), C.byref(info))
+    return {k: getattr(info, k) for k, _ in SystemInfo._fields_}
+
+
+def _np_ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _dptr(t) -> int | None:
+    if t is None:
+        return None
+    import torch
+    assert isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous(), \
+        "device tensors must be contiguous float32 CUDA tensors"
+    return t.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    import torch
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class Projector:
+    """One projection plan (replaces the reference's initDevice* + forward*GPU)."""
+
+    def __init__(self, geometry: dict, n_materials: int, interp: str = "trilinear", device: int = 0):
+        self.geometry = dict(geometry)
+        self.M = int(n_materials)
+        self.interp = interp
+        self.device = int(device)
+        self._g = make_geometry(self.geometry)
+        h = C.c_void_p()
+        call("ctfp_plan_create", C.byref(self._g), self.M, INTERP[interp], self.device, C.byref(h))
+        self._h = h
+        info = SystemInfo()
+        call("ctfp_plan_get_system_info", self._h, C.byref(info))
+        self.info = {k: getattr(info, k) for k, _ in SystemInfo._fields_}
+        self.E = 0
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ctfp_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def shape_proj(self) -> tuple[int, int, int]:
+        g = self.geometry
+        return (int(g["projNum"]), int(g["dNumV"]), int(g["dNumU"]))
+
+    @property
+    def shape_vol(self) -> tuple[int, int, int]:
+        g = self.geometry
+        return (int(g["pNumZ"]), int(g["pNumY"]), int(g["pNumX"]))
+
+    def set_interp(self, interp: str) -> None:
+        call("ctfp_plan_set_interp", self._h, INTERP[interp])
+        self.interp = interp
+
+    def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1) -> None:
+        call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta)
+
+    # -- tables -------------------------------------------------------------
+    def set_spectral_tables(self, spectrum, mu, grid=None, grid_layout: int | None = None, det_response=None,
+                            I0Val: float = 60000.0) -> None:
+        """spectrum [E]; mu [E][M] (1/mm per g/cm^3); grid [E][U] or [E][V][U];
+        det_response [E][V][U]; host numpy arrays."""
+        S = np.ascontiguousarray(spectrum, dtype=np.float32)
+        mu = np.ascontiguousarray(mu, dtype=np.float32).reshape(len(S), self.M)
+        G = None if grid is None else np.ascontiguousarray(grid, dtype=np.float32)
+        if G is not None and grid_layout is None:
+            grid_layout = capi.GRID_COLUMN if G.ndim == 2 else capi.GRID_PIXEL
+        D = None if det_response is None else np.ascontiguousarray(det_response, dtype=np.float32)
+        call("ctfp_set_spectral_tables", self._h, len(S), _np_ptr(S), _np_ptr(mu), _np_ptr(G),
+             int(grid_layout or 0), _np_ptr(D), float(I0Val))
+        self.E = len(S)
+
+    def set_tables_from_workload(self, w, device_tables: bool = True) -> None:
+        """Builds grid/scintillator tables for a physics.Workload on the device
+        and installs the spectral tables."""
+        import torch
+        E = len(w.energies)
+        U, V = int(self.geometry["dNumU"]), int(self.geometry["dNumV"])
+        G = D = None
+        layout = 0
+        if w.grid is not None:
+            ms, mi = w.grid_mu()
+            layout = w.grid_layout
+            G = build_grid_table(self.geometry, w.grid, ms, mi, layout, device=self.device).cpu().numpy()
+        if w.scint_mm is not None:
+            t = scintillator_thickness(U * V, w.scint_mm, w.scint_err_mm)
+            D = build_det_response(w.scint_mu(), torch.from_numpy(t).to(f"cuda:{self.device}"), 1.0).cpu().numpy()
+            D = D.reshape(E, V, U)
+        self.set_spectral_tables(w.spectrum(), w.mu_table(), G, layout if G is not None else 0, D, w.I0Val)
+
+    # -- compute ------------------------------------------------------------
+    def _vol_ptrs(self, volumes: Sequence):
+        assert len(volumes) == self.M, f"expected {self.M} volumes"
+        for v in volumes:
+            assert tuple(v.shape) == self.shape_vol, f"volume shape {tuple(v.shape)} != {self.shape_vol}"
+        return ptr_array([_dptr(v) for v in volumes])
+
+    def forward(self, volumes: Sequence, want_L: bool = False, out=None, stream=None) -> dict:
+        """Fused march + spectral epilogue. Returns dict(I, IAbsorb, I0[, L])."""
+        import torch
+        dev = f"cuda:{self.device}"
+        P, V, U = self.shape_proj
+        if out is None:
+            out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev),
+                   "I0": torch.empty((V, U), device=dev)}
+            if want_L:
+                out["L"] = torch.empty((P, V, U, self.M), device=dev)
+        call("ctfp_forward", self._h, self._vol_ptrs(volumes), _dptr(out.get("I")), _dptr(out.get("IAbsorb")),
+             _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
+        return out
+
+    def forward_host(self, host_volumes: Sequence[np.ndarray], out: dict | None = None) -> dict:
+        """ctfp_forward_host: host volumes in, host I/IAbsorb/I0 out."""
+        P, V, U = self.shape_proj
+        if out is None:
+            out = {"I": np.empty((P, V, U), np.float32), "IAbsorb": np.empty((P, V, U), np.float32),
+                   "I0": np.empty((V, U), np.float32)}
+        ptrs = ptr_array([_host_ptr(v) for v in host_volumes])
+        call("ctfp_forward_host", self._h, ptrs, _host_ptr(out["I"]), _host_ptr(out["IAbsorb"]),
+             _host_ptr(out.get("I0")), _stream(None))
+        return out
+
+    def line_integrals(self, volumes: Sequence, out=None, stream=None):
+        import torch
+        P, V, U = self.shape_proj
+        if out is None:
+            out = torch.empty((P, V, U, self.M), device=f"cuda:{self.device}")
+        call("ctfp_line_integrals", self._h, self._vol_ptrs(volumes), _dptr(out), _stream(stream))
+        return out
+
+    def spectral_from_L(self, L, stream=None) -> dict:
+        import torch
+        P, V, U = self.shape_proj
+        dev = f"cuda:{self.device}"
+        out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
+        call("ctfp_spectral_from_L", self._h, _dptr(L), _dptr(out["I"]), _dptr(out["IAbsorb"]), _stream(stream))
+        return out
+
+    def backward(self, L, gI=None, gIAbsorb=None, grads=None, stream=None) -> list:
+        """Adds dLoss/drho_m into grads (created as zeros if None)."""
+        import torch
+        if grads is None:
+            grads = [torch.zeros(self.shape_vol, device=f"cuda:{self.device}") for _ in range(self.M)]
+        call("ctfp_backward", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), ptr_array([_dptr(g) for g in grads]),
+             _stream(stream))
+        return grads
+
+    def line_integrals_adjoint(self, gL, grads=None, stream=None) -> list:
+        import torch
+        if grads is None:
+            grads = [torch.zeros(self.shape_vol, device=f"cuda:{self.device}") for _ in range(self.M)]
+        call("ctfp_line_integrals_adjoint", self._h, _dptr(gL), ptr_array([_dptr(g) for g in grads]),
+             _stream(stream))
+        return grads
+
+    def count_support_samples(self) -> int:
+        n = C.c_int64()
+        call("ctfp_count_support_samples", self._h, C.byref(n))
+        return int(n.value)
+
+
+def _host_ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return _np_ptr(a)
+    import torch
+    assert isinstance(a, torch.Tensor) and not a.is_cuda and a.dtype == torch.float32 and a.is_contiguous()
+    return a.data_ptr()
+
+
+def finalize_counts(I, IAbsorb, I0, stream=None) -> dict:
+    """Ipoly = floor(I) (uint32 as int32 tensor bits), IAbsPoly, proj = log(I0/Ipoly)."""
+    import torch
+    P, V, U = I.shape
+    Ip = torch.empty((P, V, U), dtype=torch.int32, device=I.device)
+    Ap = torch.empty((P, V, U), dtype=torch.int32, device=I.device)
+    proj = torch.empty((P, V, U), dtype=torch.float32, device=I.device)
+    call("ctfp_finalize_counts", V * U, P, _dptr(I), _dptr(IAbsorb), _dptr(I0), Ip.data_ptr(), Ap.data_ptr(),
+         _dptr(proj), _stream(stream))
+    return {"Ipoly": Ip, "IAbsPoly": Ap, "proj": proj}
+
+
+def sample_volume(volume, points, interp: str, stream=None):
+    """Samples volume [nz][ny][nx] at points [n][3] (x, y, z voxel coordinates)."""
+    import torch
+    nz, ny, nx = volume.shape
+    out = torch.empty(points.shape[0], device=volume.device)
+    call("ctfp_sample_volume", _dptr(volume), nx, ny, nz, INTERP[interp], _dptr(points.contiguous()),
+         points.shape[0], _dptr(out), _stream(stream))
+    return out
+
+
+def build_grid_table(geometry: dict, grid, mu_strip, mu_inter, layout: int, device: int = 0):
+    import torch
+    g = make_geometry(geometry)
+    gp = GridParams(int(grid.strip_um), int(grid.inter_um), float(grid.h_mm), float(grid.FD_mm))
+    ms = np.ascontiguousarray(mu_strip, dtype=np.float32)
+    mi = np.ascontiguousarray(mu_inter, dtype=np.float32)
+    E = len(ms)
+    shape = (E, int(geometry["dNumU"])) if layout == capi.GRID_COLUMN else \
+        (E, int(geometry["dNumV"]), int(geometry["dNumU"]))
+    out = torch.empty(shape, device=f"cuda:{device}")
+    call("ctfp_build_grid_table", C.byref(g), C.byref(gp), E, _np_ptr(ms), _np_ptr(mi), layout, _dptr(out),
+         _stream(None))
+    return out
+
+
+def scintillator_thickness(n_pix: int, thickness: float, thickness_err: float) -> np.ndarray:
+    out = np.empty(n_pix, np.float32)
+    call("ctfp_scintillator_thickness", n_pix, float(thickness), float(thickness_err), _np_ptr(out))
+    return out
+
+
+def build_det_response(mu_scint, thickness_dev, factor: float):
+    import torch
+    mu = np.ascontiguousarray(mu_scint, dtype=np.float32)
+    n = thickness_dev.numel()
+    out = torch.empty((len(mu), n), device=thickness_dev.device)
+    call("ctfp_build_det_response", len(mu), n, _np_ptr(mu), _dptr(thickness_dev), float(factor), _dptr(out),
+         _stream(None))
+    return out
+
+
+def labels_to_density(labels_dev, density: Sequence[float]):
+    import torch
+    M = len(density)
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    outs = [torch.empty(labels_dev.shape, device=labels_dev.device) for _ in range(M)]
+    call("ctfp_labels_to_density", labels_dev.data_ptr(), labels_dev.numel(), M, _np_ptr(d),
+         ptr_array([o.data_ptr() for o in outs]), _stream(None))
+    return outs

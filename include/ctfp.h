@@ -1,0 +1,255 @@
+/*
+ * ctfp.h — C ABI of the B200 polyenergetic cone-beam forward projector.
+ *
+ * This is the device boundary that replaces the reference's GPU layer
+ * (Source/CUDAFun/CBCTPolyProjGPU.cuh:33-114).  The reference exposed free
+ * C++ functions taking its structs by value and kept process-global texture
+ * state (CBCTPolyProjGPU.cu:8-10), reset the device in every init
+ * (CBCTPolyProjGPU.cu:494) and printed-and-ignored CUDA errors
+ * (CBCTPolyProjGPU.cu:55-61).  Here every call returns a ctfp_status, the
+ * device is never reset, all state lives in a plan object, and the caller owns
+ * every device buffer it passes in (volumes, outputs, checkpoints, gradients).
+ *
+ * Layouts (C order, last index fastest):
+ *   volume      [pNumZ][pNumY][pNumX]  float32, one buffer per material
+ *   projections [projNum][dNumV][dNumU] float32
+ *   I0          [dNumV][dNumU]          float32
+ *   L checkpoint[projNum][dNumV][dNumU][M] float32 (per-ray material path
+ *               integrals, g/cm^3 * mm)
+ *
+ * Streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ * All launches are asynchronous on that stream; outputs are valid after the
+ * stream is synchronised.  One plan may be used from one host thread at a time;
+ * distinct plans are independent.
+ */
+#ifndef CTFP_H
+#define CTFP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTFP_MAX_MATERIALS 4
+#define CTFP_MAX_ENERGIES 256
+
+typedef enum ctfp_status {
+    CTFP_OK = 0,
+    CTFP_INVALID_ARG = 1,
+    CTFP_OOM = 2,
+    CTFP_CUDA_ERROR = 3,
+    CTFP_TIMEOUT = 4,
+    CTFP_UNSUPPORTED = 5,
+    CTFP_NOT_READY = 6
+} ctfp_status;
+
+/* Scan geometry: the fields of CTScanParas (Source/DataType.h:33-55) that the
+ * projector reads, with the reference's names and units (mm, counts). */
+typedef struct ctfp_geometry {
+    int64_t pNumX, pNumY, pNumZ;        /* phantom voxels                        */
+    float pLengthX, pLengthY, pLengthZ; /* phantom size, mm                      */
+    int64_t projNum;                    /* views over 360 degrees                */
+    int64_t dNumU, dNumV;               /* detector columns, rows                */
+    float dSize;                        /* detector pitch, mm                    */
+    float sod, sdd;                     /* source-object, source-detector, mm    */
+    int32_t rotatedDirection;           /* +1 counter-clockwise, -1 clockwise    */
+    int32_t reserved;                   /* must be 0                             */
+} ctfp_geometry;
+
+/* Derived quantities: CTScanSystemInfo (Source/DataType.h:78-111) exactly as
+ * CBCTForwardProj::computeParas computes them in FP32
+ * (Source/CBCTForwardProj.cpp:23-62). */
+typedef struct ctfp_system_info {
+    float thetaStep, dHalfLU, dHalfLV, FOVR, FOVH;
+    float pHalfX, pHalfY, pHalfZ;
+    float pSizeX, pSizeY, pSizeZ;
+    float dx, dy, dz;
+    int64_t intNum; /* samples per ray, K */
+} ctfp_system_info;
+
+/* How a material volume is sampled at a ray point. */
+typedef enum ctfp_interp {
+    /* exact FP32 software trilinear at the reference's sample coordinates */
+    CTFP_INTERP_TRILINEAR = 0,
+    /* software trilinear with the weights quantised to 8 fractional bits, as
+     * the texture unit does for the reference's tex3D (CBCTPolyProjGPU.cu:1920) */
+    CTFP_INTERP_TEXEMU = 1,
+    /* hardware tex3D on a cudaArray, the reference's own sampler
+     * (CBCTPolyProjGPU.cu:2175-2209: border addressing, linear filter) */
+    CTFP_INTERP_TEXTURE = 2
+} ctfp_interp;
+
+/* Grid transmission table layout for ctfp_set_spectral_tables. */
+typedef enum ctfp_grid_layout {
+    CTFP_GRID_NONE = 0,   /* no anti-scatter grid: G = 1                 */
+    CTFP_GRID_COLUMN = 1, /* [E][dNumU], the reference's Grid::updataGrid */
+    CTFP_GRID_PIXEL = 2   /* [E][dNumV][dNumU], per-pixel per-energy      */
+} ctfp_grid_layout;
+
+typedef struct ctfp_plan ctfp_plan;
+
+/* ---- geometry ------------------------------------------------------------ */
+
+/* CBCTForwardProj::computeParas (Source/CBCTForwardProj.cpp:23-62). */
+ctfp_status ctfp_compute_paras(const ctfp_geometry* g, ctfp_system_info* out);
+
+/* View angle in radians, FP32 as the reference's launchers compute it
+ * (CBCTPolyProjGPU.cu:51): rotatedDirection * p * thetaStep / 180 * acosf(-1). */
+ctfp_status ctfp_view_angle(const ctfp_geometry* g, int64_t view, float* angle);
+
+/* ---- plans ---------------------------------------------------------------- */
+
+/* Replaces initDevice{,SinMat,SinMatNoResponse}{Grid,NoGrid}
+ * (CBCTPolyProjGPU.cu:478-1764) without their cudaDeviceReset, without the
+ * 3*K*U*V coordinate buffers and without the K*U*V sample buffer. */
+ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_t interp,
+                             int32_t device, ctfp_plan** out);
+/* Replaces freeDeviceMemory (CBCTPolyProjGPU.cu:1774-1797). */
+ctfp_status ctfp_plan_destroy(ctfp_plan* plan);
+ctfp_status ctfp_plan_get_system_info(const ctfp_plan* plan, ctfp_system_info* out);
+ctfp_status ctfp_plan_set_interp(ctfp_plan* plan, int32_t interp);
+/* Ray-tile shape of the march kernels: tile_u x tile_v pixels per CTA (a
+ * multiple of 32 threads, at most 256) and views_per_cta views marched by each
+ * CTA for its tile.  Set by the autotuner; defaults 32 x 8 x 1. */
+ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t tile_v, int32_t views_per_cta);
+
+/* Spectral tables, host pointers, copied into the plan.
+ *   spectrum     [E]     normalised spectrum S_e
+ *   mu           [E][M]  per-material attenuation per unit density, 1/mm per
+ *                        g/cm^3, i.e. (mu/rho)(E)/10 (PhantomObject.cpp:56,62)
+ *   grid         NULL or [E][dNumU] / [E][dNumV][dNumU] per grid_layout
+ *   det_response NULL (D = 1) or [E][dNumV][dNumU]
+ *                (CBCTForwardProj.cpp:114-120 per energy)
+ *   I0Val        photons per pixel before weighting (CTScanParas::I0Val)
+ * Builds the per-pixel energy weights W_e = I0Val*S_e*G_e*D_e and the flat
+ * field I0 = sum_e W_e (CBCTPolyForwardProjGrid.cpp:330-350). */
+ctfp_status ctfp_set_spectral_tables(ctfp_plan* plan, int32_t n_energies, const float* spectrum,
+                                     const float* mu, const float* grid, int32_t grid_layout,
+                                     const float* det_response, float I0Val);
+
+/* ---- forward -------------------------------------------------------------- */
+
+/* Per-ray material path integrals L_m = dx * sum_i interp(rho_m, x_i)
+ * (transformKernel + computeSinMatIndensityProjKernel, CBCTPolyProjGPU.cu:1902-1924,
+ * 2005-2020), written to L [projNum][dNumV][dNumU][M]. volumes: M device
+ * pointers (host array). */
+ctfp_status ctfp_line_integrals(ctfp_plan* plan, const float* const* volumes, float* L, void* stream);
+
+/* Fused ray march + spectral epilogue. Replaces the per-energy, per-view loop
+ * of forward{,SinMat,SinMatNoResponse}Proj{Grid,NoGrid}GPU (CBCTPolyProjGPU.cu:12-474)
+ * and the host sum over energies (CBCTForwardProj.cpp:65-76):
+ *   I   = sum_e W_e exp(-sum_m mu[e][m] L_m)
+ *   IAbs= sum_e W_e (1 - exp(-sum_m mu[e][m] L_m))
+ * I, IAbsorb: device [projNum][dNumV][dNumU]; I0 (device [dNumV][dNumU]) and
+ * L_ckpt (device [projNum][dNumV][dNumU][M]) may be NULL. */
+ctfp_status ctfp_forward(ctfp_plan* plan, const float* const* volumes, float* I, float* IAbsorb,
+                         float* I0, float* L_ckpt, void* stream);
+
+/* ctfp_forward with HOST buffers, the shape of the reference's per-energy
+ * launchers (CBCTPolyProjGPU.cu:12-109: host volume in, host I/IAbsorb out):
+ * copies the M host volumes to plan-owned device buffers, runs ctfp_forward and
+ * copies I, IAbsorb (host [projNum][dNumV][dNumU]) and I0 (host [dNumV][dNumU],
+ * may be NULL) back, then synchronises the stream.  Page-locked host buffers
+ * make the copies asynchronous DMA. */
+ctfp_status ctfp_forward_host(ctfp_plan* plan, const float* const* host_volumes, float* host_I,
+                              float* host_IAbsorb, float* host_I0, void* stream);
+
+/* Spectral epilogue alone from given path integrals L (e.g. the single-material
+ * path's density projection, forwardSin*Kernel, CBCTPolyProjGPU.cu:2046-2169). */
+ctfp_status ctfp_spectral_from_L(ctfp_plan* plan, const float* L, float* I, float* IAbsorb, void* stream);
+
+/* Compat outputs (CBCTForwardProj.cpp:79-90, 376-387): Ipoly = floor(I) as
+ * uint32, IAbsPoly = floor(IAbsorb), proj = logf(I0 / Ipoly). n_pix = U*V.
+ * Any output pointer may be NULL. */
+ctfp_status ctfp_finalize_counts(int64_t n_pix, int64_t n_views, const float* I, const float* IAbsorb,
+                                 const float* I0, uint32_t* Ipoly, uint32_t* IAbsPoly, float* proj,
+                                 void* stream);
+
+/* ---- adjoint (no reference counterpart) ------------------------------------ */
+
+/* Gradient of a loss with respect to each material density map, given dLoss/dI
+ * (gI) and optionally dLoss/dIAbsorb (gIAbsorb, may be NULL), both
+ * [projNum][dNumV][dNumU], and the L checkpoint written by ctfp_forward.
+ * Accumulates (+=) into g_volumes (M device pointers, same layout as volumes):
+ *   gL_m   = (gIAbs - gI) * sum_e mu[e][m] W_e exp(-sum_k mu[e][k] L_k)
+ *   g_rho_m[x] += dx * sum_{rays, i} w_i(x) gL_m     (transposed trilinear weights)
+ * In CTFP_INTERP_TEXTURE mode the transposed weights are the quantised
+ * texture weights (CTFP_INTERP_TEXEMU). */
+ctfp_status ctfp_backward(ctfp_plan* plan, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                          float* const* g_volumes, void* stream);
+
+/* Transpose of ctfp_line_integrals: g_volumes[m][x] += dx * sum w_i(x) gL[ray][m]. */
+ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float* const* g_volumes,
+                                        void* stream);
+
+/* ---- table builders on the device -------------------------------------- */
+
+/* Focused anti-scatter grid geometry, GridInfo (Source/DataType.h:57-75). */
+typedef struct ctfp_grid_params {
+    int32_t gridStripsWidth;  /* um, integer (Grid.h:6-8)  */
+    int32_t interspaceWidth;  /* um, integer               */
+    float h;                  /* grid height, mm           */
+    float FD;                 /* focal distance, mm        */
+} ctfp_grid_params;
+
+/* Grid transmission per energy, written to device memory `out`:
+ *   layout CTFP_GRID_COLUMN: [E][dNumU], the reference's 1-um discretised
+ *     focused strip grid averaged over each detector column
+ *     (Grid::defGrid/updataGrid/binning1D, Grid.cpp:76-309, 373-443), including
+ *     its quirk that an interspace takes the period-start unit's height
+ *     (Grid.cpp:115);
+ *   layout CTFP_GRID_PIXEL: [E][dNumV][dNumU], the same strip pattern with the
+ *     slant path through the grid taken from the full incidence angle of the ray
+ *     to each pixel, h * sqrt(FD^2 + d_u^2 + d_v^2) / FD (reduces to the column
+ *     table on the central row).
+ * mu_strip, mu_inter: host [E], linear attenuation in 1/mm (the mass tables
+ * times density / 10, CBCTForwardProj.cpp:196, 220).  dSize*1000 must be an
+ * integer number of um. */
+ctfp_status ctfp_build_grid_table(const ctfp_geometry* g, const ctfp_grid_params* grid, int32_t n_energies,
+                                  const float* mu_strip, const float* mu_inter, int32_t layout, float* out,
+                                  void* stream);
+
+/* Per-pixel scintillator thickness with the reference's seeded jitter
+ * (CBCTForwardProj::computePerScinThinckness, CBCTForwardProj.cpp:99-111):
+ * srand(100) and the MSVC CRT rand() the reference was built with.  Host
+ * output [n_pix]. */
+ctfp_status ctfp_scintillator_thickness(int64_t n_pix, float thickness, float thickness_err, float* out);
+
+/* Detector response per energy on the device (CBCTForwardProj::updateDetResponse,
+ * CBCTForwardProj.cpp:114-120): out[e][k] = factor * (1 - exp(-mu_scint[e] * t[k])).
+ * mu_scint: host [E] in 1/mm; thickness: device [n_pix]; out: device [E][n_pix]. */
+ctfp_status ctfp_build_det_response(int32_t n_energies, int64_t n_pix, const float* mu_scint,
+                                    const float* thickness, float factor, float* out, void* stream);
+
+/* Label map -> M density maps on the device (PhantomObject::updataLineAtten /
+ * computeDesity, PhantomObject.cpp:38-71): out[m][x] = density[m] if
+ * labels[x] == m + 1 else 0.  labels: device uint8 [n_vox]; density: host [M];
+ * out: M device pointers. */
+ctfp_status ctfp_labels_to_density(const uint8_t* labels, int64_t n_vox, int32_t n_materials,
+                                   const float* density, float* const* out, void* stream);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+
+/* Samples one volume [nz][ny][nx] at n points (device float3 array of
+ * continuous voxel coordinates, voxel i at i) with the given interp mode,
+ * border 0. Used to pin the texture emulation against the hardware sampler. */
+ctfp_status ctfp_sample_volume(const float* volume, int64_t nx, int64_t ny, int64_t nz, int32_t interp,
+                               const float* points, int64_t n, float* out, void* stream);
+
+/* Exact number of (ray, sample) pairs whose trilinear footprint touches the
+ * volume, i.e. the samples the march evaluates (others contribute exactly 0). */
+ctfp_status ctfp_count_support_samples(ctfp_plan* plan, int64_t* out);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char* ctfp_last_error_string(void);
+
+/* Library version string. */
+const char* ctfp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTFP_H */

@@ -1,0 +1,465 @@
+/*
+ * ctfp_oracle.c — FP64 CPU ORACLE for the polyenergetic cone-beam forward
+ * projection.  TEST INFRASTRUCTURE ONLY: it is the checker that tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg compare the CUDA
+ * path against.  Nothing in the product links, loads or calls it.
+ *
+ * It restates, in plain C and double precision, the reference's per-ray
+ * algorithm (DiuYao/CT_Forward_Projection):
+ *   A1  CBCTForwardProj::computeParas           Source/CBCTForwardProj.cpp:23-62 (FP32, as written)
+ *   A2  computeIntPointCoordinatesKernel        Source/CUDAFun/CBCTPolyProjGPU.cu:1813-1848
+ *   A3  transformKernel + tex3D sampling        Source/CUDAFun/CBCTPolyProjGPU.cu:1915-1920, 2198-2205
+ *   A4/A5 per-ray sum * dx                      Source/CUDAFun/CBCTPolyProjGPU.cu:1989-1995, 2014-2018
+ *   A6  single-material epilogue                Source/CUDAFun/CBCTPolyProjGPU.cu:2055-2056
+ *   A8  scintillator thickness + response       Source/CBCTForwardProj.cpp:99-120
+ *   A9  focused grid transmission               Source/Grid.cpp:76-309, 373-443
+ *   A10 energy sums, I0                         Source/CBCTForwardProj.cpp:65-76,
+ *                                               Source/CBCTPolyForwardProjGrid.cpp:330-350
+ *   A11 uint32 floor + proj                     Source/CBCTForwardProj.cpp:79-90, 376-387
+ * plus the adjoint of the march (no reference counterpart).
+ *
+ * Parity pins: the reference ships no tests, fixtures or golden outputs.  This
+ * oracle is pinned by (1) the reference's own CUDA pipeline built from its
+ * sources (oracle/build_ref.sh -> oracle/_ref/) and run on a B200 to make the
+ * committed fixtures under tests/golden/, and (2) analytic known answers
+ * (uniform slabs, zero volume, single/multi-material equivalence).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct orc_geometry {
+    int64_t pNumX, pNumY, pNumZ;
+    float pLengthX, pLengthY, pLengthZ;
+    int64_t projNum;
+    int64_t dNumU, dNumV;
+    float dSize;
+    float sod, sdd;
+    int32_t rotatedDirection;
+    int32_t reserved;
+} orc_geometry;
+
+typedef struct orc_sysinfo {
+    float thetaStep, dHalfLU, dHalfLV, FOVR, FOVH;
+    float pHalfX, pHalfY, pHalfZ;
+    float pSizeX, pSizeY, pSizeZ;
+    float dx, dy, dz;
+    int64_t intNum;
+} orc_sysinfo;
+
+enum { ORC_TRILINEAR = 0, ORC_TEXEMU = 1 };
+
+/* ------------------------------------------------------------------------ */
+/* A1: CBCTForwardProj::computeParas, FP32 arithmetic in the reference's order
+ * (CBCTForwardProj.cpp:28-60).  Built with -ffp-contract=off so that no
+ * product is fused into an add, matching an x86-64 SSE float evaluation. */
+void orc_compute_paras(const orc_geometry* g, orc_sysinfo* s)
+{
+    memset(s, 0, sizeof(*s));
+    s->thetaStep = (float)360 / (float)g->projNum;                       /* :28 */
+    s->dHalfLU = (float)g->dNumU * g->dSize / 2;                         /* :29 */
+    s->dHalfLV = (float)g->dNumV * g->dSize / 2;                         /* :30 */
+    s->FOVR = g->sod * s->dHalfLU / sqrtf(s->dHalfLU * s->dHalfLU + g->sdd * g->sdd); /* :33-34 */
+    s->FOVH = (g->sod - s->FOVR) * s->dHalfLV / g->sdd;                  /* :35-36 */
+    s->pSizeX = g->pLengthX / (float)g->pNumX;                           /* :45 */
+    s->pSizeY = g->pLengthY / (float)g->pNumY;
+    s->pSizeZ = g->pLengthZ / (float)g->pNumZ;
+    s->pHalfX = g->pLengthX / 2;                                         /* :50 */
+    s->pHalfY = g->pLengthY / 2;
+    s->pHalfZ = g->pLengthZ / 2;
+    s->dx = (float)(0.5 * s->pSizeX);                                    /* :55 */
+    s->dy = (float)(0.5 * s->pSizeY);
+    s->dz = (float)(0.5 * s->pSizeZ);
+    s->intNum = (int64_t)roundf(2 * s->FOVR / s->dx);                    /* :60 */
+}
+
+/* View angle, FP32, CBCTPolyProjGPU.cu:51 with PI = acosf(-1) (.cuh:21).
+ * The reference multiplies the int direction by a size_t view index, which for
+ * rotatedDirection = -1 wraps to ~2^64 and yields one constant angle for every
+ * view; the intended signed angle is restated here instead. */
+float orc_view_angle(const orc_geometry* g, const orc_sysinfo* s, int64_t p)
+{
+    float a = (float)p * s->thetaStep / 180.0f * acosf(-1.0f);
+    return g->rotatedDirection < 0 ? -a : a;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sample coordinates of ray (p, v, u), sample i, in continuous voxel index
+ * space (voxel j sits at j because the reference adds 0.5 to the texture
+ * coordinate, CBCTPolyProjGPU.cu:1920).  Per ray: detector position and
+ * direction cosines (.cu:1813-1829), t_i (.cu:1846), rotation and axis flips
+ * (.cu:1915-1917). */
+typedef struct ray_coef {
+    double ax, bx, ay, by, az, bz; /* c(i) = a + b * i per axis */
+} ray_coef;
+
+static void ray_setup(const orc_geometry* g, const orc_sysinfo* s, double cth, double sth, int64_t v,
+                      int64_t u, ray_coef* r)
+{
+    double dsz = g->dSize, sdd = g->sdd, sod = g->sod;
+    double detU = (double)s->dHalfLU - dsz / 2 - (double)u * dsz;
+    double detV = (double)s->dHalfLV - dsz / 2 - (double)v * dsz;
+    double R = sqrt(sdd * sdd + detU * detU + detV * detV);
+    double sinG = detV / R;
+    double cosG = sqrt(sdd * sdd + detU * detU) / R;
+    double sinB = detU / R;
+    double cosB = sqrt(sdd * sdd + detV * detV) / R;
+    double A = cosG * cosB, B = cosG * sinB, C = sinG; /* X = A t - sod, Y = B t, Z = C t */
+    double t0 = sod - (double)s->FOVR + (double)s->dx / 2, dt = s->dx;
+    /* tu = X cos - Y sin + pHalfX ; tv = -(X sin + Y cos) + pHalfY ; tw = -Z + pHalfZ */
+    double ku = A * cth - B * sth, cu = -sod * cth + s->pHalfX;
+    double kv = -(A * sth + B * cth), cv = sod * sth + s->pHalfY;
+    double kw = -C, cw = s->pHalfZ;
+    r->ax = (ku * t0 + cu) / s->pSizeX;
+    r->bx = ku * dt / s->pSizeX;
+    r->ay = (kv * t0 + cv) / s->pSizeY;
+    r->by = kv * dt / s->pSizeY;
+    r->az = (kw * t0 + cw) / s->pSizeZ;
+    r->bz = kw * dt / s->pSizeZ;
+}
+
+static inline double vox(const float* vol, int64_t nx, int64_t ny, int64_t nz, int64_t x, int64_t y, int64_t z)
+{
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return 0.0; /* border addressing */
+    return (double)vol[(z * ny + y) * nx + x];
+}
+
+/* Texture-unit weight: the fraction of x_B = x - 0.5 held with 8 fractional
+ * bits, rounded to nearest (CUDA Programming Guide, texture fetching: alpha is
+ * stored in 9-bit fixed point with 8 fractional bits, so 1.0 is exactly
+ * representable). */
+static inline double q8(double f) { return floor(f * 256.0 + 0.5) / 256.0; }
+
+/* Trilinear corner weights and base index for one sample. */
+typedef struct tri {
+    int64_t ix, iy, iz;
+    double wx, wy, wz;
+} tri;
+
+static inline void tri_weights(int mode, double cx, double cy, double cz, tri* t)
+{
+    if (mode == ORC_TEXEMU) {
+        /* the reference passes float(c + 0.5) to tex3D; the unit subtracts 0.5 */
+        double xb = (double)(float)(cx + 0.5) - 0.5;
+        double yb = (double)(float)(cy + 0.5) - 0.5;
+        double zb = (double)(float)(cz + 0.5) - 0.5;
+        double fx = floor(xb), fy = floor(yb), fz = floor(zb);
+        t->ix = (int64_t)fx; t->iy = (int64_t)fy; t->iz = (int64_t)fz;
+        t->wx = q8(xb - fx); t->wy = q8(yb - fy); t->wz = q8(zb - fz);
+    } else {
+        double fx = floor(cx), fy = floor(cy), fz = floor(cz);
+        t->ix = (int64_t)fx; t->iy = (int64_t)fy; t->iz = (int64_t)fz;
+        t->wx = cx - fx; t->wy = cy - fy; t->wz = cz - fz;
+    }
+}
+
+static inline double sample(const float* vol, int64_t nx, int64_t ny, int64_t nz, const tri* t)
+{
+    double s = 0.0;
+    for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                double w = (dx ? t->wx : 1.0 - t->wx) * (dy ? t->wy : 1.0 - t->wy) * (dz ? t->wz : 1.0 - t->wz);
+                s += w * vox(vol, nx, ny, nz, t->ix + dx, t->iy + dy, t->iz + dz);
+            }
+    return s;
+}
+
+static void ray_index(const orc_geometry* g, int64_t id, int64_t* p, int64_t* v, int64_t* u)
+{
+    *u = id % g->dNumU;
+    *v = (id / g->dNumU) % g->dNumV;
+    *p = id / (g->dNumU * g->dNumV);
+}
+
+/* ------------------------------------------------------------------------ */
+/* A2-A5: L[r][m] = dx * sum_{i<K} interp(vol_m, c_i) for the rays listed in
+ * ray_ids (NULL = all projNum*dNumV*dNumU rays in [p][v][u] order). */
+void orc_line_integrals(const orc_geometry* g, int M, const float* const* vols, int mode, int64_t nrays,
+                        const int64_t* ray_ids, double* L)
+{
+    orc_sysinfo s;
+    orc_compute_paras(g, &s);
+    const int64_t K = s.intNum, nx = g->pNumX, ny = g->pNumY, nz = g->pNumZ;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrays; r++) {
+        int64_t p, v, u;
+        ray_index(g, ray_ids ? ray_ids[r] : r, &p, &v, &u);
+        double th = (double)orc_view_angle(g, &s, p);
+        ray_coef c;
+        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        double acc[8] = {0};
+        for (int64_t i = 0; i < K; i++) {
+            double cx = c.ax + c.bx * (double)i, cy = c.ay + c.by * (double)i, cz = c.az + c.bz * (double)i;
+            if (!(cx > -1.0 && cy > -1.0 && cz > -1.0 && cx < (double)nx && cy < (double)ny && cz < (double)nz)) {
+                /* every corner outside the volume; exact zero for TRILINEAR.  For
+                 * TEXEMU the float rounding of c + 0.5 can only move c by far
+                 * less than one voxel, so a sample outside (-1.01, n + 0.01) is
+                 * still all-border. */
+                if (mode != ORC_TEXEMU || !(cx > -1.01 && cy > -1.01 && cz > -1.01 && cx < nx + 0.01 &&
+                                           cy < ny + 0.01 && cz < nz + 0.01))
+                    continue;
+            }
+            tri t;
+            tri_weights(mode, cx, cy, cz, &t);
+            for (int m = 0; m < M; m++) acc[m] += sample(vols[m], nx, ny, nz, &t);
+        }
+        for (int m = 0; m < M; m++) L[r * M + m] = (double)s.dx * acc[m];
+    }
+}
+
+/* A10 weights: W[e][v][u] = I0Val * S_e * G_e * D_e in double.
+ * grid: NULL, [E][U] (layout 1) or [E][V][U] (layout 2); det: NULL or [E][V][U]. */
+void orc_energy_weights(const orc_geometry* g, int E, const float* spectrum, const float* grid, int grid_layout,
+                        const float* det, double I0Val, double* W)
+{
+    const int64_t U = g->dNumU, V = g->dNumV;
+    for (int e = 0; e < E; e++)
+        for (int64_t v = 0; v < V; v++)
+            for (int64_t u = 0; u < U; u++) {
+                double w = I0Val * (double)spectrum[e];
+                if (grid && grid_layout == 1) w *= (double)grid[(int64_t)e * U + u];
+                if (grid && grid_layout == 2) w *= (double)grid[((int64_t)e * V + v) * U + u];
+                if (det) w *= (double)det[((int64_t)e * V + v) * U + u];
+                W[((int64_t)e * V + v) * U + u] = w;
+            }
+}
+
+/* A4/A6/A10: I = sum_e W_e exp(-sum_m mu[e][m] L_m), IAbs = sum_e W_e (1 - exp(...)). */
+void orc_spectral(const orc_geometry* g, int M, int E, const float* mu, const double* W, int64_t nrays,
+                  const int64_t* ray_ids, const double* L, double* I, double* IAbs)
+{
+    const int64_t U = g->dNumU, V = g->dNumV;
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < nrays; r++) {
+        int64_t p, v, u;
+        ray_index(g, ray_ids ? ray_ids[r] : r, &p, &v, &u);
+        double si = 0.0, sa = 0.0;
+        for (int e = 0; e < E; e++) {
+            double att = 0.0;
+            for (int m = 0; m < M; m++) att += (double)mu[e * M + m] * L[r * M + m];
+            double w = W[((int64_t)e * V + v) * U + u];
+            si += w * exp(-att);
+            sa += w * -expm1(-att);
+        }
+        if (I) I[r] = si;
+        if (IAbs) IAbs[r] = sa;
+    }
+}
+
+void orc_flat_field(const orc_geometry* g, int E, const double* W, double* I0)
+{
+    const int64_t n = g->dNumU * g->dNumV;
+    for (int64_t k = 0; k < n; k++) {
+        double s = 0.0;
+        for (int e = 0; e < E; e++) s += W[(int64_t)e * n + k];
+        I0[k] = s;
+    }
+}
+
+/* Full forward for a ray subset. */
+void orc_forward(const orc_geometry* g, int M, const float* const* vols, int mode, int E, const float* mu,
+                 const double* W, int64_t nrays, const int64_t* ray_ids, double* I, double* IAbs, double* L)
+{
+    int own = (L == NULL);
+    if (own) L = (double*)malloc(sizeof(double) * (size_t)nrays * (size_t)M);
+    orc_line_integrals(g, M, vols, mode, nrays, ray_ids, L);
+    orc_spectral(g, M, E, mu, W, nrays, ray_ids, L, I, IAbs);
+    if (own) free(L);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Adjoint.  gL_m = (gIAbs - gI) * sum_e mu[e][m] W_e exp(-sum_k mu[e][k] L_k);
+ * g_vol_m[x] += dx * gL_m * sum_i w_i(x).  All rays (ray_ids NULL) or a list.
+ * g_vols: M double arrays of nx*ny*nz, accumulated.  Serial: small cases. */
+void orc_backward(const orc_geometry* g, int M, int mode, int E, const float* mu, const double* W,
+                  int64_t nrays, const int64_t* ray_ids, const double* L, const double* gI,
+                  const double* gIAbs, double* const* g_vols)
+{
+    orc_sysinfo s;
+    orc_compute_paras(g, &s);
+    const int64_t K = s.intNum, nx = g->pNumX, ny = g->pNumY, nz = g->pNumZ, U = g->dNumU, V = g->dNumV;
+    for (int64_t r = 0; r < nrays; r++) {
+        int64_t p, v, u;
+        ray_index(g, ray_ids ? ray_ids[r] : r, &p, &v, &u);
+        double gl[8] = {0};
+        double gdiff = (gIAbs ? gIAbs[r] : 0.0) - (gI ? gI[r] : 0.0);
+        for (int e = 0; e < E; e++) {
+            double att = 0.0;
+            for (int m = 0; m < M; m++) att += (double)mu[e * M + m] * L[r * M + m];
+            double Ie = W[((int64_t)e * V + v) * U + u] * exp(-att);
+            for (int m = 0; m < M; m++) gl[m] += (double)mu[e * M + m] * Ie;
+        }
+        for (int m = 0; m < M; m++) gl[m] *= gdiff * (double)s.dx;
+        double th = (double)orc_view_angle(g, &s, p);
+        ray_coef c;
+        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        for (int64_t i = 0; i < K; i++) {
+            double cx = c.ax + c.bx * (double)i, cy = c.ay + c.by * (double)i, cz = c.az + c.bz * (double)i;
+            if (!(cx > -1.01 && cy > -1.01 && cz > -1.01 && cx < nx + 0.01 && cy < ny + 0.01 && cz < nz + 0.01))
+                continue;
+            tri t;
+            tri_weights(mode, cx, cy, cz, &t);
+            for (int dz = 0; dz < 2; dz++)
+                for (int dy = 0; dy < 2; dy++)
+                    for (int dx = 0; dx < 2; dx++) {
+                        int64_t x = t.ix + dx, y = t.iy + dy, z = t.iz + dz;
+                        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) continue;
+                        double w = (dx ? t.wx : 1.0 - t.wx) * (dy ? t.wy : 1.0 - t.wy) * (dz ? t.wz : 1.0 - t.wz);
+                        for (int m = 0; m < M; m++) g_vols[m][(z * ny + y) * nx + x] += w * gl[m];
+                    }
+        }
+    }
+}
+
+/* Transpose of orc_line_integrals: g_vol_m[x] += dx * gL[r][m] * sum_i w_i(x). */
+void orc_line_integrals_adjoint(const orc_geometry* g, int M, int mode, int64_t nrays, const int64_t* ray_ids,
+                                const double* gL, double* const* g_vols)
+{
+    orc_sysinfo s;
+    orc_compute_paras(g, &s);
+    const int64_t K = s.intNum, nx = g->pNumX, ny = g->pNumY, nz = g->pNumZ;
+    for (int64_t r = 0; r < nrays; r++) {
+        int64_t p, v, u;
+        ray_index(g, ray_ids ? ray_ids[r] : r, &p, &v, &u);
+        double th = (double)orc_view_angle(g, &s, p);
+        ray_coef c;
+        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        for (int64_t i = 0; i < K; i++) {
+            double cx = c.ax + c.bx * (double)i, cy = c.ay + c.by * (double)i, cz = c.az + c.bz * (double)i;
+            if (!(cx > -1.01 && cy > -1.01 && cz > -1.01 && cx < nx + 0.01 && cy < ny + 0.01 && cz < nz + 0.01))
+                continue;
+            tri t;
+            tri_weights(mode, cx, cy, cz, &t);
+            for (int dz = 0; dz < 2; dz++)
+                for (int dy = 0; dy < 2; dy++)
+                    for (int dx = 0; dx < 2; dx++) {
+                        int64_t x = t.ix + dx, y = t.iy + dy, z = t.iz + dz;
+                        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) continue;
+                        double w = (dx ? t.wx : 1.0 - t.wx) * (dy ? t.wy : 1.0 - t.wy) * (dz ? t.wz : 1.0 - t.wz);
+                        for (int m = 0; m < M; m++)
+                            g_vols[m][(z * ny + y) * nx + x] += (double)s.dx * gL[r * M + m] * w;
+                    }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* A11: Ipoly = floorf(I) as uint32; proj = logf(I0 / Ipoly) (FP32, as the
+ * reference's host code). */
+void orc_finalize(int64_t n_pix, int64_t n_views, const float* I, const float* I0, uint32_t* Ipoly, float* proj)
+{
+    for (int64_t k = 0; k < n_pix * n_views; k++) {
+        Ipoly[k] = (uint32_t)floorf(I[k]);
+        if (proj) proj[k] = logf(I0[k % n_pix] / (float)Ipoly[k]);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* A8: per-pixel CsI thickness with the reference's seeded jitter
+ * (CBCTForwardProj.cpp:99-111).  The reference was built with MSVC, whose CRT
+ * rand() is the LCG state = state*214013 + 2531011, output (state>>16)&0x7fff,
+ * seeded with srand(100). */
+void orc_scint_thickness(int64_t n_pix, float thickness, float thickness_err, float* out)
+{
+    uint32_t state = 100u;
+    int beg = (int)(-thickness_err * 10000);
+    int endd = (int)(thickness_err * 10000);
+    for (int64_t i = 0; i < n_pix; i++) {
+        state = state * 214013u + 2531011u;
+        int r = (int)((state >> 16) & 0x7fff);
+        float err = -thickness_err + (float)(r % (endd - beg + 1)) / 10000.0f;
+        out[i] = thickness + err;
+    }
+}
+
+/* A8: D[e][k] = factor * (1 - expf(-mu_e * t_k)) (CBCTForwardProj.cpp:114-120),
+ * mu_e in 1/mm (the CsI table * density / 10, CBCTForwardProj.cpp:247). */
+void orc_det_response(int E, int64_t n_pix, const float* mu_scint, const float* thick, float factor, float* D)
+{
+    for (int e = 0; e < E; e++)
+        for (int64_t k = 0; k < n_pix; k++)
+            D[(int64_t)e * n_pix + k] = factor * (1.0f - expf(-mu_scint[e] * thick[k]));
+}
+
+/* A9: focused anti-scatter grid, 1-um discretisation, per-column mean.
+ * Grid::defGrid + Grid::updataGrid + Grid::binning1D (Grid.cpp:373-443, 76-309)
+ * for one energy.  Widths in um (integers), h and FD in mm, dSize in mm,
+ * attenuation in 1/mm.  Arithmetic precision as the reference (float units,
+ * double bin sums). */
+int orc_grid_column(int64_t dNumU, float dSize_mm, int strip_um, int inter_um, float h_mm, float FD_mm,
+                    float mu_strip_mm, float mu_inter_mm, float* grid_out)
+{
+    size_t dSize = (size_t)(float)(dSize_mm * 1000);    /* CBCTPolyForwardProjGrid.cpp:291 -> Grid.h:126 */
+    size_t N = (size_t)dNumU * dSize;                   /* Grid.cpp:376 */
+    float h = h_mm * 1000, FD = FD_mm * 1000;           /* Grid.cpp:43-44 */
+    float ms = mu_strip_mm / 1000, mi = mu_inter_mm / 1000; /* Grid.cpp:410-411 */
+    int period = inter_um + strip_um;                    /* Grid.cpp:386 */
+    if (dSize == 0 || N < (size_t)inter_um + 2 || period <= 0) return -1;
+    float* unitH = (float*)malloc(N * sizeof(float));
+    float* g1 = (float*)malloc(N * sizeof(float));
+    for (size_t i = 0; i < N; i++) {                     /* Grid.cpp:76-87 */
+        float dc = (float)((double)i + 0.5 - (double)((float)N / 2));
+        unitH[i] = h / FD * sqrtf(FD * FD + dc * dc);
+    }
+    for (size_t i = 0; i < N; i++) g1[i] = 0.0f;
+    int uOdd = (int)(N % 2), iOdd = inter_um % 2;
+    size_t c = N / 2;
+    long start;
+    if (!uOdd && !iOdd) {                                /* uEdE Grid.cpp:90-130 */
+        for (size_t i = c - 1; i > c - 1 - (size_t)(inter_um / 2); i--) g1[i] = expf(-mi * unitH[i]);
+        start = (long)(c - 1 - (size_t)(inter_um / 2));
+    } else if (!uOdd && iOdd) {                          /* uEdO Grid.cpp:133-174 */
+        g1[c] = expf(-mi * unitH[c]);
+        for (size_t i = c - 1; i > c - 1 - (size_t)(inter_um / 2); i--) g1[i] = expf(-mi * unitH[i]);
+        start = (long)(c - 1 - (size_t)(inter_um / 2));
+    } else if (uOdd && !iOdd) {                          /* uOdE Grid.cpp:177-219 */
+        for (size_t i = c; i > c - (size_t)(inter_um / 2); i--) g1[i] = expf(-mi * unitH[i]);
+        start = (long)(c - (size_t)(inter_um / 2));
+    } else {                                             /* uOdO Grid.cpp:222-270 */
+        g1[c] = expf(-mi * unitH[c]);
+        for (size_t i = c - 1; i > c - 1 - (size_t)(inter_um / 2); i--) g1[i] = expf(-mi * unitH[i]);
+        start = (long)(c - 1 - (size_t)(inter_um / 2));
+    }
+    for (long i = start; i >= 0; i -= period) {
+        for (int k = 0; k < strip_um; k++) {
+            if (i - k < 0) break;
+            g1[i - k] = expf(-ms * unitH[i - k]);
+        }
+        for (int k = 0; k < inter_um; k++) {
+            if (i - strip_um - k < 0) break;
+            /* interspace uses the period-start unit's height (Grid.cpp:115) */
+            g1[i - strip_um - k] = expf(-mi * unitH[i]);
+        }
+    }
+    if (!uOdd && !iOdd) {
+        for (size_t i = c; i < N; i++) g1[i] = g1[N - i - 1];  /* Grid.cpp:126-129 */
+    } else if (!uOdd && iOdd) {
+        for (size_t i = c + 1; i < N; i++) g1[i] = g1[N - i];  /* Grid.cpp:170-173 */
+    } else if (uOdd && !iOdd) {
+        for (size_t i = c + 1; i < N; i++) g1[i] = g1[N - i];  /* Grid.cpp:214-217 */
+    } else {
+        for (size_t i = c + 1; i < N; i++) g1[i] = g1[N - i - 1]; /* Grid.cpp:260-263 */
+    }
+    for (size_t i = 0; i < N; i += dSize) {              /* binning1D Grid.cpp:297-309 */
+        double sum = 0.0;
+        for (size_t j = 0; j < dSize; j++) sum += g1[i + j];
+        grid_out[i / dSize] = (float)(sum / (double)dSize);
+    }
+    free(unitH);
+    free(g1);
+    return 0;
+}
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,115 @@
+"""The hand-written adjoint (no reference counterpart): dot-product test,
+FP64 oracle adjoint, central finite differences of an FP64 loss."""
+import numpy as np
+import pytest
+import torch
+
+from ct_forward_projection_b200 import Projector
+from oracle import oracle as O
+from tests.conftest import random_volumes, small_geometry, spectral_setup
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(vols):
+    return [torch.from_numpy(v).cuda() for v in vols]
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("M", [1, 2, 3])
+def test_line_integral_adjoint_dot_product(cuda_ok, mode, M):
+    # <A x, y> = <x, A^T y>, both sides accumulated in FP64
+    d = small_geometry(n=(18, 14, 11), views=5, U=21, V=13)
+    x = random_volumes(d, M, 50 + M)
+    rng = np.random.RandomState(M)
+    with Projector(d, M, mode) as pr:
+        Ax = pr.line_integrals(to_dev(x)).double().cpu().numpy()
+        y = rng.normal(size=Ax.shape).astype(np.float32)
+        g = pr.line_integrals_adjoint(torch.from_numpy(y).cuda())
+        torch.cuda.synchronize()
+    lhs = float(np.sum(Ax * y.astype(np.float64)))
+    rhs = float(sum(np.sum(g[m].double().cpu().numpy() * x[m].astype(np.float64)) for m in range(M)))
+    assert abs(lhs - rhs) / max(abs(lhs), 1e-30) < 1e-5
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+def test_line_integral_adjoint_vs_oracle(cuda_ok, mode):
+    d = small_geometry(n=12, views=4, U=14, V=9)
+    M = 2
+    rng = np.random.RandomState(2)
+    gL = rng.normal(size=(d["projNum"] * d["dNumV"] * d["dNumU"], M)).astype(np.float32)
+    with Projector(d, M, mode) as pr:
+        g = pr.line_integrals_adjoint(torch.from_numpy(gL.reshape(d["projNum"], d["dNumV"], d["dNumU"], M)).cuda())
+        torch.cuda.synchronize()
+    ref = O.line_integrals_adjoint(d, gL, M, O.TRILINEAR if mode == "trilinear" else O.TEXEMU)
+    for m in range(M):
+        a = g[m].double().cpu().numpy()
+        scale = np.max(np.abs(ref[m]))
+        assert np.max(np.abs(a - ref[m])) / scale < (1e-5 if mode == "trilinear" else 1e-3)
+
+
+def test_backward_vs_oracle(cuda_ok):
+    d = small_geometry(n=14, views=4, U=16, V=10)
+    M = 2
+    vols = random_volumes(d, M, 31)
+    S, mu, G, D = spectral_setup(d, M, 9, 4)
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    rng = np.random.RandomState(7)
+    n = d["projNum"] * d["dNumV"] * d["dNumU"]
+    gI = rng.normal(size=n).astype(np.float32)
+    gA = rng.normal(size=n).astype(np.float32)
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        f = pr.forward(to_dev(vols), want_L=True)
+        shp = f["I"].shape
+        g = pr.backward(f["L"], torch.from_numpy(gI).cuda().view(shp), torch.from_numpy(gA).cuda().view(shp))
+        torch.cuda.synchronize()
+        L = f["L"].double().cpu().numpy().reshape(n, M)
+    ref = O.backward(d, mu, W, L, gI, gA, O.TRILINEAR)
+    for m in range(M):
+        a = g[m].double().cpu().numpy()
+        assert np.max(np.abs(a - ref[m])) / np.max(np.abs(ref[m])) < 1e-4
+
+
+def test_backward_central_differences(cuda_ok):
+    # loss = sum (log I - log I_t)^2; gradient from the GPU adjoint against FP64
+    # central differences of the oracle loss on 64 seeded voxels
+    d = small_geometry(n=10, views=3, U=12, V=8)
+    M = 2
+    vols = random_volumes(d, M, 61)
+    S, mu, G, D = spectral_setup(d, M, 7, 6)
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    rng = np.random.RandomState(9)
+    target = O.forward(d, [v * np.float32(0.97) for v in vols], mu, W)["I"]
+    logt = np.log(target)
+
+    def loss(vs):
+        I = O.forward(d, vs, mu, W)["I"]
+        return float(np.sum((np.log(I) - logt) ** 2))
+
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        f = pr.forward(to_dev(vols), want_L=True)
+        I = f["I"].double()
+        gI = (2.0 * (torch.log(I) - torch.from_numpy(logt).cuda().view(I.shape)) / I).float()
+        g = pr.backward(f["L"], gI)
+        torch.cuda.synchronize()
+    g = [x.double().cpu().numpy() for x in g]
+    shape = vols[0].shape
+    worst = 0.0
+    for k in range(64):
+        m = k % M
+        idx = tuple(rng.randint(0, s) for s in shape)
+        h = 1e-3
+        vp = [v.astype(np.float64).copy() for v in vols]
+        vm = [v.astype(np.float64).copy() for v in vols]
+        vp[m][idx] += h
+        vm[m][idx] -= h
+        fd = (loss([v.astype(np.float32) for v in vp]) - loss([v.astype(np.float32) for v in vm])) / (2 * h)
+        # the perturbation itself is rounded to float32; use the realised step
+        hp = np.float32(vols[m][idx] + np.float32(h)) - vols[m][idx]
+        hm = vols[m][idx] - np.float32(vols[m][idx] - np.float32(h))
+        fd = fd * 2 * h / (float(hp) + float(hm))
+        scale = max(abs(fd), 1e-3 * np.max(np.abs(g[m])))
+        worst = max(worst, abs(g[m][idx] - fd) / scale)
+    assert worst < 2e-2

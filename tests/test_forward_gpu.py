@@ -1,0 +1,218 @@
+"""Parity of the CUDA forward path (through the C ABI) with the FP64 oracle.
+
+Tolerances (relative, per pixel, against the FP64 oracle on the same inputs):
+  software trilinear (CTFP_INTERP_TRILINEAR)     1e-5
+  texture emulation  (CTFP_INTERP_TEXEMU)        1e-4   (8-bit weights flip on
+                     FP32-vs-FP64 coordinate differences at quantisation edges)
+  hardware texture   (CTFP_INTERP_TEXTURE)       1e-4 against the emulation
+"""
+import numpy as np
+import pytest
+import torch
+
+from ct_forward_projection_b200 import Projector, finalize_counts, sample_volume
+from oracle import oracle as O
+from tests.conftest import random_volumes, small_geometry, spectral_setup
+
+pytestmark = pytest.mark.gpu
+
+RTOL_TRI = 1e-5
+RTOL_TEX = 1e-4
+
+
+def rel_err(x, ref):
+    x = np.asarray(x, np.float64).reshape(-1)
+    ref = np.asarray(ref, np.float64).reshape(-1)
+    den = np.maximum(np.abs(ref), 1e-30)
+    return float(np.max(np.abs(x - ref) / den)) if ref.size else 0.0
+
+
+def rel_err_scaled(x, ref, floor_frac=1e-6):
+    """Relative error with a floor of floor_frac * max|ref| (for L, where rays
+    that graze the volume have tiny path integrals)."""
+    x = np.asarray(x, np.float64).reshape(-1)
+    ref = np.asarray(ref, np.float64).reshape(-1)
+    den = np.maximum(np.abs(ref), floor_frac * max(np.max(np.abs(ref)), 1e-30))
+    return float(np.max(np.abs(x - ref) / den)) if ref.size else 0.0
+
+
+def to_dev(vols):
+    return [torch.from_numpy(v).cuda() for v in vols]
+
+
+GEOMS = [
+    dict(n=24, views=6, U=20, V=12),
+    dict(n=(20, 16, 12), views=5, U=17, V=11),
+    dict(n=16, views=4, U=33, V=9, rot=-1),
+    dict(n=(9, 23, 14), views=3, U=8, V=40),
+]
+
+
+@pytest.mark.parametrize("gi", range(len(GEOMS)))
+@pytest.mark.parametrize("M", [1, 2, 3, 4])
+def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M):
+    d = small_geometry(**GEOMS[gi])
+    vols = random_volumes(d, M, 100 + gi * 7 + M)
+    with Projector(d, M, "trilinear") as pr:
+        L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1, M)
+    Lref = O.line_integrals(d, vols, O.TRILINEAR)
+    assert rel_err_scaled(L, Lref) < RTOL_TRI
+
+
+@pytest.mark.parametrize("gi", range(len(GEOMS)))
+@pytest.mark.parametrize("M", [1, 2, 4])
+def test_forward_trilinear_vs_oracle(cuda_ok, gi, M):
+    d = small_geometry(**GEOMS[gi])
+    vols = random_volumes(d, M, 200 + gi + M)
+    S, mu, G, D = spectral_setup(d, M, 17, 5 + gi)
+    W = O.energy_weights(d, S, G, 2, D, 60000.0)
+    ref = O.forward(d, vols, mu, W, O.TRILINEAR)
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        out = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    assert rel_err(out["I"].cpu(), ref["I"]) < RTOL_TRI
+    assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TRI
+    assert rel_err(out["I0"].cpu(), W.sum(axis=0)) < 1e-6
+    assert rel_err_scaled(out["L"].cpu().numpy().reshape(-1, M), ref["L"]) < RTOL_TRI
+
+
+@pytest.mark.parametrize("layout", [0, 1, 2])
+def test_forward_grid_layouts_and_no_response(cuda_ok, layout):
+    d = small_geometry(n=16, views=4, U=24, V=10)
+    M = 2
+    vols = random_volumes(d, M, 77)
+    rng = np.random.RandomState(3)
+    E = 9
+    S = rng.uniform(0.1, 1, E).astype(np.float32)
+    mu = rng.uniform(0.01, 0.05, (E, M)).astype(np.float32)
+    G = None if layout == 0 else (rng.uniform(0.5, 1, (E, 24)) if layout == 1 else
+                                  rng.uniform(0.5, 1, (E, 10, 24))).astype(np.float32)
+    W = O.energy_weights(d, S, G, layout, None, 1234.0)
+    ref = O.forward(d, vols, mu, W)
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, layout, None, 1234.0)
+        out = pr.forward(to_dev(vols))
+        torch.cuda.synchronize()
+    assert rel_err(out["I"].cpu(), ref["I"]) < RTOL_TRI
+    assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TRI
+
+
+@pytest.mark.parametrize("M", [1, 2, 3])
+def test_forward_texemu_vs_oracle(cuda_ok, M):
+    d = small_geometry(n=20, views=5, U=24, V=14)
+    vols = random_volumes(d, M, 300 + M)
+    S, mu, G, D = spectral_setup(d, M, 11, 9)
+    W = O.energy_weights(d, S, G, 2, D, 60000.0)
+    ref = O.forward(d, vols, mu, W, O.TEXEMU)
+    with Projector(d, M, "texemu") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        out = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    assert rel_err(out["I"].cpu(), ref["I"]) < RTOL_TEX
+    assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TEX
+
+
+@pytest.mark.parametrize("M", [1, 2, 4])
+def test_hardware_texture_vs_emulation(cuda_ok, M):
+    d = small_geometry(n=20, views=5, U=24, V=14)
+    vols = to_dev(random_volumes(d, M, 400 + M))
+    S, mu, G, D = spectral_setup(d, M, 11, 19)
+    outs = {}
+    for mode in ("texemu", "texture"):
+        with Projector(d, M, mode) as pr:
+            pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+            outs[mode] = pr.forward(vols, want_L=True)
+            torch.cuda.synchronize()
+    assert rel_err(outs["texture"]["I"].cpu(), outs["texemu"]["I"].cpu()) < RTOL_TEX
+    assert rel_err_scaled(outs["texture"]["L"].cpu(), outs["texemu"]["L"].cpu()) < RTOL_TEX
+
+
+def test_texture_weight_rounding_pinned(cuda_ok):
+    # the hardware sampler at random points against the 8-bit emulation, per
+    # sample; pins the weight quantisation rule the emulation uses
+    rng = np.random.RandomState(0)
+    vol = torch.from_numpy(rng.uniform(-1, 1, (6, 7, 8)).astype(np.float32)).cuda()
+    pts = rng.uniform(-1.5, 8.5, (20000, 3)).astype(np.float32)
+    pts[:5000] = np.round(pts[:5000] * 512) / 512  # exact quantisation edges
+    pts_d = torch.from_numpy(pts).cuda()
+    hw = sample_volume(vol, pts_d, "texture").cpu().numpy()
+    em = sample_volume(vol, pts_d, "texemu").cpu().numpy()
+    tri = sample_volume(vol, pts_d, "trilinear").cpu().numpy()
+    assert np.max(np.abs(hw - em)) < 2e-5
+    assert np.max(np.abs(hw - tri)) < 8e-3
+
+
+def test_zero_volume_is_flat_field(cuda_ok):
+    d = small_geometry()
+    S, mu, G, D = spectral_setup(d, 2, 5, 1)
+    with Projector(d, 2, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        z = [torch.zeros(pr.shape_vol, device="cuda") for _ in range(2)]
+        out = pr.forward(z)
+        torch.cuda.synchronize()
+    I0 = out["I0"].cpu().numpy()
+    assert np.array_equal(out["I"].cpu().numpy(), np.broadcast_to(I0, out["I"].shape))
+    assert float(out["IAbsorb"].abs().max()) == 0.0
+
+
+def test_spectral_from_L_matches_fused(cuda_ok):
+    d = small_geometry()
+    vols = to_dev(random_volumes(d, 3, 5))
+    S, mu, G, D = spectral_setup(d, 3, 13, 2)
+    with Projector(d, 3, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        f = pr.forward(vols, want_L=True)
+        s = pr.spectral_from_L(f["L"])
+        torch.cuda.synchronize()
+    assert torch.equal(f["I"], s["I"]) and torch.equal(f["IAbsorb"], s["IAbsorb"])
+
+
+def test_forward_host_matches_device(cuda_ok):
+    d = small_geometry()
+    vols = random_volumes(d, 2, 8)
+    S, mu, G, D = spectral_setup(d, 2, 7, 3)
+    with Projector(d, 2, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        dev = pr.forward(to_dev(vols))
+        torch.cuda.synchronize()
+        host = pr.forward_host(vols)
+    assert np.array_equal(host["I"], dev["I"].cpu().numpy())
+    assert np.array_equal(host["IAbsorb"], dev["IAbsorb"].cpu().numpy())
+    assert np.array_equal(host["I0"], dev["I0"].cpu().numpy())
+
+
+def test_finalize_counts_vs_oracle(cuda_ok):
+    rng = np.random.RandomState(1)
+    I = (rng.uniform(0, 5e4, (3, 4, 5)).astype(np.float32))
+    I[0, 0, :2] = [0.3, 0.0]
+    I0 = rng.uniform(5e4, 6e4, (4, 5)).astype(np.float32)
+    A = rng.uniform(0, 5e4, (3, 4, 5)).astype(np.float32)
+    out = finalize_counts(torch.from_numpy(I).cuda(), torch.from_numpy(A).cuda(), torch.from_numpy(I0).cuda())
+    Ip, proj = O.finalize(I, I0)
+    assert np.array_equal(out["Ipoly"].cpu().numpy().view(np.uint32), Ip)
+    assert np.array_equal(out["IAbsPoly"].cpu().numpy().view(np.uint32), np.floor(A).astype(np.uint32))
+    p = out["proj"].cpu().numpy()
+    fin = np.isfinite(proj)
+    assert np.array_equal(np.isinf(p), ~fin)
+    assert np.max(np.abs(p[fin] - proj[fin])) < 2e-6
+
+
+@pytest.mark.parametrize("U,V,P", [(1, 1, 1), (1, 7, 2), (33, 1, 3)])
+def test_degenerate_detectors(cuda_ok, U, V, P):
+    d = small_geometry(n=10, views=P, U=U, V=V, pitch=1.5)
+    vols = random_volumes(d, 1, 4)
+    with Projector(d, 1, "trilinear") as pr:
+        L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1, 1)
+    assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
+
+
+def test_rays_missing_volume_are_zero(cuda_ok):
+    # a detector offset so far that every ray passes beside the volume
+    d = small_geometry(n=8, views=2, U=6, V=6, length=8.0, pitch=60.0)
+    vols = [np.ones((8, 8, 8), np.float32)]
+    with Projector(d, 1, "trilinear") as pr:
+        L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1)
+    ref = O.line_integrals(d, vols).reshape(-1)
+    assert np.array_equal(L == 0, ref == 0)
+    assert rel_err_scaled(L, ref) < RTOL_TRI
