@@ -76,6 +76,8 @@ _SIGNATURES = {
     "ctfp_scintillator_thickness": (C.c_int, [C.c_int64, C.c_float, C.c_float, _P]),
     "ctfp_build_det_response": (C.c_int, [C.c_int32, C.c_int64, _P, _P, C.c_float, _P, _P]),
     "ctfp_labels_to_density": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, _P]),
+    "ctfp_forward_noalloc": (C.c_int, [C.POINTER(Geometry), C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
+                                       _P, C.c_float, _P, _P, _P, _P, _P]),
     "ctfp_last_error_string": (C.c_char_p, []),
     "ctfp_version": (C.c_char_p, []),
 }

@@ -184,6 +184,39 @@ ctfp_status ctfp_backward(ctfp_plan* plan, const float* L_ckpt, const float* gI,
 ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float* const* g_volumes,
                                         void* stream);
 
+/* ---- forward without device allocation -------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running inside a host framework that owns all device memory through its
+ * own pool, real-time loops that must not allocate after start-up, or processes
+ * held to a fixed memory budget on a shared GPU.  ctfp_forward needs a plan, and
+ * a plan allocates its tables; this entry point allocates nothing.
+ *
+ * It runs the same fused march + spectral epilogue as ctfp_forward on the
+ * calling thread's current device.  The caller passes every input and output:
+ * spectrum [E] and mu [E][M] (host), grid (device: NULL, [E][dNumU] or
+ * [E][dNumV][dNumU] per grid_layout), det_response (device, NULL or
+ * [E][dNumV][dNumU]), volumes (M device pointers), I and IAbsorb (device
+ * [projNum][dNumV][dNumU]) and I0 (device [dNumV][dNumU], may be NULL).  The
+ * energy weights I0Val*S*G*D are formed per ray instead of being tabulated.
+ *
+ * Its scratch (per-view trigonometry, the attenuation and spectrum tables) is a
+ * fixed array of CTFP_NOALLOC_SCRATCH_BYTES in the library's device module,
+ * which every GPU that loads the library holds until the process exits.  Limits:
+ * projNum <= CTFP_NOALLOC_MAX_VIEWS, n_energies <= CTFP_MAX_ENERGIES,
+ * n_materials <= CTFP_MAX_MATERIALS; larger sizes return CTFP_INVALID_ARG.
+ * interp must be CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU (the hardware
+ * texture needs a cudaArray).  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls on a device share the array and it keeps the last call's
+ * contents: calls whose work overlaps on the GPU (different streams or threads)
+ * race on it and must be serialised by the caller. */
+#define CTFP_NOALLOC_MAX_VIEWS 8192
+#define CTFP_NOALLOC_SCRATCH_BYTES (136 * 1024)
+ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_materials, int32_t interp, int32_t n_energies,
+                                 const float* spectrum, const float* mu, const float* grid, int32_t grid_layout,
+                                 const float* det_response, float I0Val, const float* const* volumes, float* I,
+                                 float* IAbsorb, float* I0, void* stream);
+
 /* ---- table builders on the device -------------------------------------- */
 
 /* Focused anti-scatter grid geometry, GridInfo (Source/DataType.h:57-75). */
