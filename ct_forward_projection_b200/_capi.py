@@ -18,6 +18,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOU
 
 INTERP_TRILINEAR, INTERP_TEXEMU, INTERP_TEXTURE = 0, 1, 2
 GRID_NONE, GRID_COLUMN, GRID_PIXEL = 0, 1, 2
+SAMPLER_GLOBAL, SAMPLER_LAYERED = 1, 2
 MAX_MATERIALS = 4
 
 
@@ -60,6 +61,7 @@ _SIGNATURES = {
     "ctfp_plan_destroy": (C.c_int, [_P]),
     "ctfp_plan_get_system_info": (C.c_int, [_P, C.POINTER(SystemInfo)]),
     "ctfp_plan_set_interp": (C.c_int, [_P, C.c_int32]),
+    "ctfp_plan_set_sampler": (C.c_int, [_P, C.c_int32]),
     "ctfp_plan_set_launch_shape": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "ctfp_set_spectral_tables": (C.c_int, [_P, C.c_int32, _P, _P, _P, C.c_int32, _P, C.c_float]),
     "ctfp_line_integrals": (C.c_int, [_P, _P, _P, _P]),

@@ -25,6 +25,7 @@ struct ctfp_plan {
     int device = 0;
     GeomParams gp{};
     double2* d_trig = nullptr;  // [P] (cos, sin) of the FP32 view angles
+    float2* d_trigf = nullptr;  // [P] the same rounded to FP32 (compat samplers)
     // spectral tables
     int E = 0;
     bool spectral_ready = false;
@@ -34,6 +35,10 @@ struct ctfp_plan {
     // texture mode
     cudaArray_t arr[kMaxM] = {};
     cudaTextureObject_t tex[kMaxM] = {};
+    // layered-gather sampler for the software modes
+    int sampler = SAMPLER_LAYERED;
+    cudaArray_t larr[kMaxM] = {};
+    cudaTextureObject_t ltex[kMaxM] = {};
     LaunchShape shape{};
     unsigned long long* d_count = nullptr;
     // staging for ctfp_forward_host
@@ -167,24 +172,57 @@ ctfp_status make_textures(ctfp_plan* p)
     return CTFP_OK;
 }
 
+// One layered 2D array per material (a layer per z slice), read by tld4.
+ctfp_status make_layered(ctfp_plan* p)
+{
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaExtent ext = make_cudaExtent((size_t)p->geom.pNumX, (size_t)p->geom.pNumY, (size_t)p->geom.pNumZ);
+    for (int m = 0; m < p->M; m++) {
+        if (p->larr[m]) continue;
+        CTFP_CUDA(cudaMalloc3DArray(&p->larr[m], &cd, ext, cudaArrayLayered));
+        cudaResourceDesc rd;
+        std::memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = p->larr[m];
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        CTFP_CUDA(cudaCreateTextureObject(&p->ltex[m], &rd, &td, nullptr));
+    }
+    return CTFP_OK;
+}
+
 void free_textures(ctfp_plan* p)
 {
     for (int m = 0; m < kMaxM; m++) {
         if (p->tex[m]) cudaDestroyTextureObject(p->tex[m]);
         if (p->arr[m]) cudaFreeArray(p->arr[m]);
+        if (p->ltex[m]) cudaDestroyTextureObject(p->ltex[m]);
+        if (p->larr[m]) cudaFreeArray(p->larr[m]);
         p->tex[m] = 0;
         p->arr[m] = nullptr;
+        p->ltex[m] = 0;
+        p->larr[m] = nullptr;
     }
 }
 
+bool uses_layered(const ctfp_plan* p) { return p->interp != INTERP_TEXTURE && p->sampler == SAMPLER_LAYERED; }
+
+// Refreshes the plan's arrays (3D for TEXTURE, layered for the layered
+// sampler) from the caller's linear volumes; no-op for the global sampler.
 ctfp_status upload_textures(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
 {
+    const bool tex3d = p->interp == INTERP_TEXTURE;
+    if (!tex3d && !uses_layered(p)) return CTFP_OK;
     for (int m = 0; m < p->M; m++) {
         cudaMemcpy3DParms cp;
         std::memset(&cp, 0, sizeof(cp));
         cp.srcPtr = make_cudaPitchedPtr((void*)volumes[m], (size_t)p->geom.pNumX * sizeof(float),
                                         (size_t)p->geom.pNumX, (size_t)p->geom.pNumY);
-        cp.dstArray = p->arr[m];
+        cp.dstArray = tex3d ? p->arr[m] : p->larr[m];
         cp.extent = make_cudaExtent((size_t)p->geom.pNumX, (size_t)p->geom.pNumY, (size_t)p->geom.pNumZ);
         cp.kind = cudaMemcpyDeviceToDevice;
         CTFP_CUDA(cudaMemcpy3DAsync(&cp, st));
@@ -202,7 +240,10 @@ MarchParams base_params(const ctfp_plan* p)
     prm.W = p->d_W;
     prm.view0 = 0;
     prm.n_views = (int)p->geom.projNum;
-    for (int m = 0; m < kMaxM; m++) prm.tex[m] = p->tex[m];
+    for (int m = 0; m < kMaxM; m++) {
+        prm.tex[m] = p->tex[m];
+        prm.ltex[m] = p->ltex[m];
+    }
     return prm;
 }
 
@@ -273,18 +314,34 @@ ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_
     gp.pHalfX = info.pHalfX; gp.pHalfY = info.pHalfY; gp.pHalfZ = info.pHalfZ;
     gp.pSizeX = info.pSizeX; gp.pSizeY = info.pSizeY; gp.pSizeZ = info.pSizeZ;
     std::vector<double2> trig((size_t)g->projNum);
+    std::vector<float2> trigf((size_t)g->projNum);
     for (int64_t k = 0; k < g->projNum; k++) {
         const double a = (double)view_angle(g, &info, k);
         trig[(size_t)k] = make_double2(std::cos(a), std::sin(a));
+        trigf[(size_t)k] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     cudaError_t e = cudaMalloc(&p->d_trig, sizeof(double2) * trig.size());
     if (e == cudaSuccess) e = cudaMemcpy(p->d_trig, trig.data(), sizeof(double2) * trig.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_trigf, sizeof(float2) * trigf.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->d_trigf, trigf.data(), sizeof(float2) * trigf.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_count, sizeof(unsigned long long));
     if (e != cudaSuccess) {
         ctfp_plan_destroy(p);
         return cuda_fail(e, "plan allocation");
     }
     gp.trig = p->d_trig;
+    gp.trigf = p->d_trigf;
+    // layered 2D textures hold at most 2048 layers
+    if (g->pNumZ > 2048) p->sampler = SAMPLER_GLOBAL;
+    if (uses_layered(p)) {
+        st = make_layered(p);
+        if (st != CTFP_OK) {
+            std::string msg = g_last_error;
+            ctfp_plan_destroy(p);
+            return fail(st, msg);
+        }
+    }
     if (interp == INTERP_TEXTURE) {
         st = make_textures(p);
         if (st != CTFP_OK) {
@@ -303,6 +360,7 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     DeviceScope ds(p->device);
     free_textures(p);
     cudaFree(p->d_trig);
+    cudaFree(p->d_trigf);
     cudaFree(p->d_mu);
     cudaFree(p->d_W);
     cudaFree(p->d_I0);
@@ -331,6 +389,20 @@ ctfp_status ctfp_plan_set_interp(ctfp_plan* p, int32_t interp)
         if (st != CTFP_OK) return st;
     }
     p->interp = interp;
+    if (uses_layered(p)) return make_layered(p);
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_plan_set_sampler(ctfp_plan* p, int32_t sampler)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    if (sampler != CTFP_SAMPLER_GLOBAL && sampler != CTFP_SAMPLER_LAYERED)
+        return fail(CTFP_INVALID_ARG, "unknown sampler");
+    if (sampler == CTFP_SAMPLER_LAYERED && p->geom.pNumZ > 2048)
+        return fail(CTFP_UNSUPPORTED, "layered sampler holds at most 2048 z slices");
+    DeviceScope ds(p->device);
+    p->sampler = sampler;
+    if (uses_layered(p)) return make_layered(p);
     return CTFP_OK;
 }
 
@@ -385,11 +457,9 @@ ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float
     MarchParams prm = base_params(p);
     for (int m = 0; m < p->M; m++) prm.vol[m] = volumes[m];
     prm.L = L;
-    if (p->interp == INTERP_TEXTURE) {
-        st = upload_textures(p, volumes, s);
-        if (st != CTFP_OK) return st;
-    }
-    CTFP_CUDA(launch_forward(prm, p->M, p->interp, false, p->shape, s));
+    st = upload_textures(p, volumes, s);
+    if (st != CTFP_OK) return st;
+    CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, false, p->shape, s));
     return CTFP_OK;
 }
 
@@ -407,11 +477,9 @@ ctfp_status ctfp_forward(ctfp_plan* p, const float* const* volumes, float* I, fl
     prm.I = I;
     prm.IAbs = IAbsorb;
     prm.L = L_ckpt;
-    if (p->interp == INTERP_TEXTURE) {
-        st = upload_textures(p, volumes, s);
-        if (st != CTFP_OK) return st;
-    }
-    CTFP_CUDA(launch_forward(prm, p->M, p->interp, true, p->shape, s));
+    st = upload_textures(p, volumes, s);
+    if (st != CTFP_OK) return st;
+    CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
     if (I0)
         CTFP_CUDA(cudaMemcpyAsync(I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
                                   cudaMemcpyDeviceToDevice, s));
@@ -570,6 +638,7 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 const GeomParams& plan_geom(const ctfp_plan* p) { return p->gp; }
 int plan_materials(const ctfp_plan* p) { return p->M; }
 int plan_interp(const ctfp_plan* p) { return p->interp; }
+int plan_sampler(const ctfp_plan* p) { return p->sampler; }
 int plan_device(const ctfp_plan* p) { return p->device; }
 int plan_energies(const ctfp_plan* p) { return p->spectral_ready ? p->E : 0; }
 const float* plan_mu(const ctfp_plan* p) { return p->d_mu; }

@@ -16,6 +16,8 @@
 namespace ctfp {
 
 enum { INTERP_TRILINEAR = 0, INTERP_TEXEMU = 1, INTERP_TEXTURE = 2 };
+// Where the software samplers (TRILINEAR, TEXEMU) read their 8 corners.
+enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2 };
 constexpr int kMaxM = 4;
 
 // Scalar geometry shared by every ray of one problem.
@@ -26,6 +28,7 @@ struct GeomParams {
     float dHalfLU, dHalfLV, dSize, sod, sdd, FOVR, dx;
     float pHalfX, pHalfY, pHalfZ, pSizeX, pSizeY, pSizeZ;
     const double2* trig;     // per view (cos, sin) of the FP32 view angle
+    const float2* trigf;     // the same, rounded to FP32 (compat samplers)
 };
 
 // One ray's sample segment: coordinates c(i) = a + b*i in FP64, evaluated
@@ -91,46 +94,151 @@ __device__ __forceinline__ RaySeg ray_segment(const GeomParams& g, int p, int v,
     return s;
 }
 
-// Trilinear footprint of one sample: base corner and weights.
+// The reference's own FP32 sample coordinates, for the samplers that
+// reproduce its texture fetch (TEXEMU, TEXTURE): the FP32 operations of
+// computeIntPointCoordinatesKernel and transformKernel
+// (CBCTPolyProjGPU.cu:1813-1848, 1915-1920), with explicit IEEE intrinsics so
+// every rounding is fixed, cos/sin of the FP32 view angle correctly rounded,
+// and fused multiply-adds where the reference's build fuses them (determined
+// from its outputs on grazing rays): detU/detV = fma(-u, dSize, dHalf - dSize/2),
+// t = fma(i, dx, t0), X = fma(cosG cosB, t, -sod), tu = fma(X, c, -(Y s)) +
+// pHalfX, tv = -fma(X, s, Y c) + pHalfY.  Rays that graze the volume have path
+// integrals that move by percents with 1e-5-voxel coordinate changes, so only
+// this arithmetic reproduces the reference's outputs there.
+struct RayRef32 {
+    float cgcb, cgsb, sinG;  // direction cosines (.cu:1825-1829, 1846-1848)
+    float c, s;              // cos, sin of the view angle
+    float t0;                // sod - FOVR + dx / 2
+};
+
+__device__ __forceinline__ RayRef32 ray_ref32(const GeomParams& g, int p, int v, int u)
+{
+    const float half = __fdiv_rn(g.dSize, 2.0f);
+    const float detU = __fmaf_rn(-(float)u, g.dSize, __fsub_rn(g.dHalfLU, half));
+    const float detV = __fmaf_rn(-(float)v, g.dSize, __fsub_rn(g.dHalfLV, half));
+    const float s2 = __fmul_rn(g.sdd, g.sdd), u2 = __fmul_rn(detU, detU), v2 = __fmul_rn(detV, detV);
+    const float R = __fsqrt_rn(__fadd_rn(__fadd_rn(s2, u2), v2));
+    RayRef32 r;
+    r.sinG = __fdiv_rn(detV, R);
+    const float cosG = __fdiv_rn(__fsqrt_rn(__fadd_rn(s2, u2)), R);
+    const float sinB = __fdiv_rn(detU, R);
+    const float cosB = __fdiv_rn(__fsqrt_rn(__fadd_rn(s2, v2)), R);
+    r.cgcb = __fmul_rn(cosG, cosB);
+    r.cgsb = __fmul_rn(cosG, sinB);
+    const float2 cs = g.trigf[p];
+    r.c = cs.x;
+    r.s = cs.y;
+    r.t0 = __fadd_rn(__fsub_rn(g.sod, g.FOVR), __fdiv_rn(g.dx, 2.0f));
+    return r;
+}
+
+// tex3D coordinates (voxel index + 0.5) of sample i.
+__device__ __forceinline__ float3 ref32_coords(const GeomParams& g, const RayRef32& r, int i)
+{
+    const float t = __fmaf_rn((float)i, g.dx, r.t0);
+    const float X = __fmaf_rn(r.cgcb, t, -g.sod);
+    const float Y = __fmul_rn(r.cgsb, t);
+    const float Z = __fmul_rn(r.sinG, t);
+    const float tu = __fadd_rn(__fmaf_rn(X, r.c, -__fmul_rn(Y, r.s)), g.pHalfX);
+    const float tv = __fadd_rn(-__fmaf_rn(X, r.s, __fmul_rn(Y, r.c)), g.pHalfY);
+    const float tw = __fadd_rn(-Z, g.pHalfZ);
+    return make_float3(__fadd_rn(__fdiv_rn(tu, g.pSizeX), 0.5f), __fadd_rn(__fdiv_rn(tv, g.pSizeY), 0.5f),
+                       __fadd_rn(__fdiv_rn(tw, g.pSizeZ), 0.5f));
+}
+
+// Trilinear footprint of one sample: base corner, the weights of the upper
+// corners (w) and of the lower corners (u = 1 - w).  Both are formed before
+// rounding to FP32, so a corner weight near 0 on either side keeps its
+// relative accuracy (1 - w computed from a rounded w near 1 would not).
 struct Corner {
     int ix, iy, iz;
     float wx, wy, wz;
+    float ux, uy, uz;
+    int qx, qy, qz;  // TEXEMU: the texture unit's 8-bit fractions (0..255)
 };
 
-// Weight of the texture unit's linear filter for x_B = x - 0.5, where x is the
-// FP32 coordinate handed to tex3D: the fraction held with 8 fractional bits.
-__device__ __forceinline__ float tex_weight(float xb, float fl)
+// The texture unit's 8 corner weights (in 1/256) for 8-bit fractions A (x),
+// B (y), C (z), measured on the B200 with single-corner tex3D probes (exact
+// over 3e4 random points): per z slice with Z = C or 256 - C, the x split
+// p1 = round_half_up(A Z / 256), p0 = Z - p1; then the y split of each,
+// upper-y weight round_half_up(B p1 / 256) for x = 1 and round_half_down(B p0 /
+// 256) for x = 0, lower-y weight the remainder.  Weights always sum to 256.
+// Index k = dz*4 + dy*2 + dx.
+__device__ __forceinline__ void texunit_weights(int A, int B, int C, float* w)
 {
-    return floorf((xb - fl) * 256.0f + 0.5f) * (1.0f / 256.0f);
+#pragma unroll
+    for (int dz = 0; dz < 2; dz++) {
+        const int Z = dz ? C : 256 - C;
+        const int p1 = (A * Z + 128) >> 8;
+        const int p0 = Z - p1;
+        const int w11 = (B * p1 + 128) >> 8;
+        const int w01 = (B * p0 + 127) >> 8;
+        w[dz * 4 + 0] = (float)(p0 - w01) * (1.0f / 256.0f);
+        w[dz * 4 + 1] = (float)(p1 - w11) * (1.0f / 256.0f);
+        w[dz * 4 + 2] = (float)w01 * (1.0f / 256.0f);
+        w[dz * 4 + 3] = (float)w11 * (1.0f / 256.0f);
+    }
+}
+
+// Interpolates the 8 corner values v[k] (k = dz*4 + dy*2 + dx).
+template <int MODE>
+__device__ __forceinline__ float interp8(const Corner& c, const float* v)
+{
+    if (MODE == 1 /* INTERP_TEXEMU */) {
+        float w[8];
+        texunit_weights(c.qx, c.qy, c.qz, w);
+        float s = w[0] * v[0];
+#pragma unroll
+        for (int k = 1; k < 8; k++) s = fmaf(w[k], v[k], s);
+        return s;
+    }
+    const float a0 = fmaf(v[1], c.wx, v[0] * c.ux), a1 = fmaf(v[3], c.wx, v[2] * c.ux);
+    const float a2 = fmaf(v[5], c.wx, v[4] * c.ux), a3 = fmaf(v[7], c.wx, v[6] * c.ux);
+    const float b0 = fmaf(a1, c.wy, a0 * c.uy), b1 = fmaf(a3, c.wy, a2 * c.uy);
+    return fmaf(b1, c.wz, b0 * c.uz);
+}
+
+// The texture unit's fixed-point coordinate for the FP32 coordinate x handed
+// to tex3D: X = round_half_up((x - 0.5) * 256); base texel X >> 8, fraction
+// X & 255 in 1/256 (measured on the B200 with in-bounds tex3D sweeps and
+// single-corner probes: exact over 3e5 + 3e4 points, edges included).
+// x * 256 - 127.5 is exact in FP32 for |x| < 2^15.
+__device__ __forceinline__ int tex_fixed(float x) { return (int)floorf(fmaf(x, 256.0f, -127.5f)); }
+
+// Texture-unit footprint at the FP32 tex3D coordinate (x, y, z) = index + 0.5.
+__device__ __forceinline__ Corner corner_tex(float3 x)
+{
+    Corner c = {};
+    const int X = tex_fixed(x.x), Y = tex_fixed(x.y), Z = tex_fixed(x.z);
+    c.ix = X >> 8; c.iy = Y >> 8; c.iz = Z >> 8;
+    c.qx = X & 255; c.qy = Y & 255; c.qz = Z & 255;
+    return c;
 }
 
 // Footprint at the FP64 coordinate (cx, cy, cz).  TRILINEAR: exact fraction
 // of the FP64 coordinate, rounded once to FP32.  TEXEMU: the texture unit's
-// view of the FP32 coordinate float(c + 0.5) that tex3D receives.
+// fixed-point view of the FP32 coordinate float(c + 0.5) that tex3D receives.
 template <int MODE>
 __device__ __forceinline__ Corner corner_of(double cx, double cy, double cz)
 {
-    Corner c;
+    Corner c = {};
     if (MODE == INTERP_TRILINEAR) {
         const double fx = floor(cx), fy = floor(cy), fz = floor(cz);
         c.ix = (int)fx; c.iy = (int)fy; c.iz = (int)fz;
         c.wx = (float)(cx - fx); c.wy = (float)(cy - fy); c.wz = (float)(cz - fz);
+        c.ux = (float)((fx + 1.0) - cx); c.uy = (float)((fy + 1.0) - cy); c.uz = (float)((fz + 1.0) - cz);
     } else {
-        const float xb = (float)(cx + 0.5) - 0.5f, yb = (float)(cy + 0.5) - 0.5f, zb = (float)(cz + 0.5) - 0.5f;
-        const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-        c.ix = (int)fx; c.iy = (int)fy; c.iz = (int)fz;
-        c.wx = tex_weight(xb, fx);
-        c.wy = tex_weight(yb, fy);
-        c.wz = tex_weight(zb, fz);
+        const int X = tex_fixed((float)(cx + 0.5)), Y = tex_fixed((float)(cy + 0.5)), Z = tex_fixed((float)(cz + 0.5));
+        c.ix = X >> 8; c.iy = Y >> 8; c.iz = Z >> 8;
+        c.qx = X & 255; c.qy = Y & 255; c.qz = Z & 255;
     }
     return c;
 }
 
-__device__ __forceinline__ float lerpf(float a, float b, float w) { return fmaf(w, b - a, a); }
 
 // Loads the 8 corners of M volumes for one footprint and interpolates.
 // Corners outside the volume read as 0 (cudaAddressModeBorder, .cu:2200-2202).
-template <int M>
+template <int M, int MODE>
 __device__ __forceinline__ void gather_interp(const float* const* __restrict__ vol, int nx, int ny, int nz,
                                               const Corner& c, float* out)
 {
@@ -142,13 +250,9 @@ __device__ __forceinline__ void gather_interp(const float* const* __restrict__ v
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const float* __restrict__ q = vol[m] + base;
-            const float v000 = __ldg(q), v100 = __ldg(q + 1);
-            const float v010 = __ldg(q + nx), v110 = __ldg(q + nx + 1);
-            const float v001 = __ldg(q + nxy), v101 = __ldg(q + nxy + 1);
-            const float v011 = __ldg(q + nxy + nx), v111 = __ldg(q + nxy + nx + 1);
-            const float a0 = lerpf(v000, v100, c.wx), a1 = lerpf(v010, v110, c.wx);
-            const float a2 = lerpf(v001, v101, c.wx), a3 = lerpf(v011, v111, c.wx);
-            out[m] = lerpf(lerpf(a0, a1, c.wy), lerpf(a2, a3, c.wy), c.wz);
+            const float v[8] = {__ldg(q), __ldg(q + 1), __ldg(q + nx), __ldg(q + nx + 1),
+                                __ldg(q + nxy), __ldg(q + nxy + 1), __ldg(q + nxy + nx), __ldg(q + nxy + nx + 1)};
+            out[m] = interp8<MODE>(c, v);
         }
     } else {
         const bool x0 = (unsigned)c.ix < (unsigned)nx, x1 = (unsigned)(c.ix + 1) < (unsigned)nx;
@@ -157,32 +261,70 @@ __device__ __forceinline__ void gather_interp(const float* const* __restrict__ v
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const float* __restrict__ q = vol[m];
-            const float v000 = (x0 && y0 && z0) ? __ldg(q + base) : 0.f;
-            const float v100 = (x1 && y0 && z0) ? __ldg(q + base + 1) : 0.f;
-            const float v010 = (x0 && y1 && z0) ? __ldg(q + base + nx) : 0.f;
-            const float v110 = (x1 && y1 && z0) ? __ldg(q + base + nx + 1) : 0.f;
-            const float v001 = (x0 && y0 && z1) ? __ldg(q + base + nxy) : 0.f;
-            const float v101 = (x1 && y0 && z1) ? __ldg(q + base + nxy + 1) : 0.f;
-            const float v011 = (x0 && y1 && z1) ? __ldg(q + base + nxy + nx) : 0.f;
-            const float v111 = (x1 && y1 && z1) ? __ldg(q + base + nxy + nx + 1) : 0.f;
-            const float a0 = lerpf(v000, v100, c.wx), a1 = lerpf(v010, v110, c.wx);
-            const float a2 = lerpf(v001, v101, c.wx), a3 = lerpf(v011, v111, c.wx);
-            out[m] = lerpf(lerpf(a0, a1, c.wy), lerpf(a2, a3, c.wy), c.wz);
+            const float v[8] = {(x0 && y0 && z0) ? __ldg(q + base) : 0.f,
+                                (x1 && y0 && z0) ? __ldg(q + base + 1) : 0.f,
+                                (x0 && y1 && z0) ? __ldg(q + base + nx) : 0.f,
+                                (x1 && y1 && z0) ? __ldg(q + base + nx + 1) : 0.f,
+                                (x0 && y0 && z1) ? __ldg(q + base + nxy) : 0.f,
+                                (x1 && y0 && z1) ? __ldg(q + base + nxy + 1) : 0.f,
+                                (x0 && y1 && z1) ? __ldg(q + base + nxy + nx) : 0.f,
+                                (x1 && y1 && z1) ? __ldg(q + base + nxy + nx + 1) : 0.f};
+            out[m] = interp8<MODE>(c, v);
         }
     }
 }
 
-// Scatters w * g[m] into the 8 corners of M gradient volumes (transposed
-// trilinear weights), skipping corners outside the volume.
-template <int M>
+// Four texels of the 2x2 footprint with lower corner (ix, iy) in one layer
+// of a layered 2D texture (tld4, PTX "texture gather").  The coordinate is the
+// footprint's centre, ix + 1 (x_B = ix + 0.5), so the unit's own 8-bit
+// coordinate rounding cannot move the footprint.  Returned in gather order:
+// x = (ix, iy+1), y = (ix+1, iy+1), z = (ix+1, iy), w = (ix, iy).  Border
+// addressing reads 0 outside the layer.
+__device__ __forceinline__ float4 gather_layer(cudaTextureObject_t t, int layer, int ix, int iy)
+{
+    float4 r;
+    const float x = (float)ix + 1.0f, y = (float)iy + 1.0f;
+    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(t), "r"(layer), "f"(x), "f"(y), "f"(y));
+    return r;
+}
+
+// The 8 corners of M volumes held as layered 2D textures (one layer per z
+// slice): two gathers per material.  Layers outside [0, nz) read as 0 here,
+// since layer indices are clamped, not bordered, by the unit.
+template <int M, int MODE>
+__device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, int nz, const Corner& c, float* out)
+{
+    const bool z0ok = (unsigned)c.iz < (unsigned)nz, z1ok = (unsigned)(c.iz + 1) < (unsigned)nz;
+    const int l0 = z0ok ? c.iz : 0, l1 = z1ok ? c.iz + 1 : 0;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        float4 a = gather_layer(ltex[m], l0, c.ix, c.iy);
+        float4 b = gather_layer(ltex[m], l1, c.ix, c.iy);
+        if (!z0ok) a = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!z1ok) b = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float v[8] = {a.w, a.z, a.x, a.y, b.w, b.z, b.x, b.y};
+        out[m] = interp8<MODE>(c, v);
+    }
+}
+
+// Scatters w_k * g[m] into the 8 corners of M gradient volumes (the
+// transposed interpolation weights), skipping corners outside the volume.
+template <int M, int MODE>
 __device__ __forceinline__ void scatter_interp(float* const* __restrict__ gvol, int nx, int ny, int nz,
                                                const Corner& c, const float* g)
 {
     const int nxy = nx * ny;
     const int base = (c.iz * ny + c.iy) * nx + c.ix;
-    const float ux = 1.f - c.wx, uy = 1.f - c.wy, uz = 1.f - c.wz;
-    const float w[8] = {ux * uy * uz, c.wx * uy * uz, ux * c.wy * uz, c.wx * c.wy * uz,
-                        ux * uy * c.wz, c.wx * uy * c.wz, ux * c.wy * c.wz, c.wx * c.wy * c.wz};
+    float w[8];
+    if (MODE == 1 /* INTERP_TEXEMU */) {
+        texunit_weights(c.qx, c.qy, c.qz, w);
+    } else {
+        const float ux = c.ux, uy = c.uy, uz = c.uz;
+        w[0] = ux * uy * uz; w[1] = c.wx * uy * uz; w[2] = ux * c.wy * uz; w[3] = c.wx * c.wy * uz;
+        w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
+    }
     const int off[8] = {0, 1, nx, nx + 1, nxy, nxy + 1, nxy + nx, nxy + nx + 1};
 #pragma unroll
     for (int k = 0; k < 8; k++) {

@@ -15,35 +15,48 @@ namespace ctfp {
 
 namespace {
 
-template <int M, int MODE>
-__device__ __forceinline__ void sample_point(const MarchParams& prm, double cx, double cy, double cz, float* val)
+template <int M, int MODE, int SAMPLER>
+__device__ __forceinline__ void sample_corner(const MarchParams& prm, const Corner& c, float* val)
 {
-    if (MODE == INTERP_TEXTURE) {
-        // the reference's own fetch: tex3D(c + 0.5) on a border/linear texture
-        const float tx = (float)(cx + 0.5), ty = (float)(cy + 0.5), tz = (float)(cz + 0.5);
-#pragma unroll
-        for (int m = 0; m < M; m++) val[m] = tex3D<float>(prm.tex[m], tx, ty, tz);
-    } else {
-        const Corner c = corner_of<MODE>(cx, cy, cz);
-        gather_interp<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, val);
-    }
+    if (SAMPLER == SAMPLER_LAYERED) gather4_interp<M, MODE>(prm.ltex, prm.g.nz, c, val);
+    else gather_interp<M, MODE>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, val);
 }
 
-// L_m for one ray, compensated FP32 sum times dx.
-template <int M, int MODE>
+// L_m for one ray, compensated FP32 sum times dx.  TRILINEAR samples at FP64
+// coordinates; the compat samplers at the reference's FP32 coordinates.
+template <int M, int MODE, int SAMPLER>
 __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, int u, float* L)
 {
     const RaySeg s = ray_segment(prm.g, p, v, u);
     float acc[M], cmp[M];
 #pragma unroll
     for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+    if (MODE == INTERP_TRILINEAR) {
 #pragma unroll 2
-    for (int i = s.i0; i < s.i1; i++) {
-        const double t = (double)i;
-        float val[M];
-        sample_point<M, MODE>(prm, fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az), val);
+        for (int i = s.i0; i < s.i1; i++) {
+            const double t = (double)i;
+            float val[M];
+            sample_corner<M, MODE, SAMPLER>(
+                prm, corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az)), val);
 #pragma unroll
-        for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+        }
+    } else {
+        const RayRef32 r = ray_ref32(prm.g, p, v, u);
+#pragma unroll 2
+        for (int i = s.i0; i < s.i1; i++) {
+            const float3 x = ref32_coords(prm.g, r, i);
+            float val[M];
+            if (MODE == INTERP_TEXTURE) {
+                // the reference's own fetch: tex3D on a border/linear texture
+#pragma unroll
+                for (int m = 0; m < M; m++) val[m] = tex3D<float>(prm.tex[m], x.x, x.y, x.z);
+            } else {
+                sample_corner<M, MODE, SAMPLER>(prm, corner_tex(x), val);
+            }
+#pragma unroll
+            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+        }
     }
 #pragma unroll
     for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
@@ -119,7 +132,7 @@ __device__ __forceinline__ void load_L(const float* L, int64_t ray, float* l)
 }
 
 // K1+K2. Grid: x = pixel tiles along u, y = along v, z = view groups.
-template <int M, int MODE, bool SPECTRAL>
+template <int M, int MODE, int SAMPLER, bool SPECTRAL>
 __global__ void __launch_bounds__(256) k_forward(const MarchParams prm)
 {
     extern __shared__ float s_mu[];
@@ -134,7 +147,7 @@ __global__ void __launch_bounds__(256) k_forward(const MarchParams prm)
         const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
         if (p >= pend) break;
         float L[M];
-        march_ray<M, MODE>(prm, p, v, u, L);
+        march_ray<M, MODE, SAMPLER>(prm, p, v, u, L);
         const int64_t ray = (int64_t)p * npix + pix;
         if (prm.L) store_L<M>(prm.L, ray, L);
         if (SPECTRAL) {
@@ -210,11 +223,18 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
         for (int m = 0; m < M; m++) any |= (g[m] != 0.f);
         if (!any) continue;
         const RaySeg s = ray_segment(prm.g, p, v, u);
-        for (int i = s.i0; i < s.i1; i++) {
-            const double t = (double)i;
-            const Corner c = corner_of<MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(
-                fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
-            scatter_interp<M>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
+        if (MODE == INTERP_TRILINEAR) {
+            for (int i = s.i0; i < s.i1; i++) {
+                const double t = (double)i;
+                const Corner c = corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+                scatter_interp<M, INTERP_TRILINEAR>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
+            }
+        } else {
+            // transpose of the texture-unit sampler at the reference's FP32 coordinates
+            const RayRef32 r = ray_ref32(prm.g, p, v, u);
+            for (int i = s.i0; i < s.i1; i++)
+                scatter_interp<M, INTERP_TEXEMU>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz,
+                                                 corner_tex(ref32_coords(prm.g, r, i)), g);
         }
     }
 }
@@ -265,9 +285,10 @@ __global__ void k_sample_points(const float* vol, cudaTextureObject_t tex, int n
             val = tex3D<float>(tex, (float)(cx + 0.5), (float)(cy + 0.5), (float)(cz + 0.5));
         } else {
             const float* vp[1] = {vol};
-            const Corner c = interp == INTERP_TEXEMU ? corner_of<INTERP_TEXEMU>(cx, cy, cz)
-                                                     : corner_of<INTERP_TRILINEAR>(cx, cy, cz);
-            gather_interp<1>(vp, nx, ny, nz, c, &val);
+            if (interp == INTERP_TEXEMU)
+                gather_interp<1, INTERP_TEXEMU>(vp, nx, ny, nz, corner_of<INTERP_TEXEMU>(cx, cy, cz), &val);
+            else
+                gather_interp<1, INTERP_TRILINEAR>(vp, nx, ny, nz, corner_of<INTERP_TRILINEAR>(cx, cy, cz), &val);
         }
         out[k] = val;
     }
@@ -295,22 +316,28 @@ __global__ void k_count_support(const GeomParams g, unsigned long long* out)
     if ((threadIdx.x & 31) == 0) atomicAdd(out, n);
 }
 
-template <int M, int MODE>
+template <int M, int MODE, int SAMPLER>
 cudaError_t fwd_dispatch_spec(const MarchParams& prm, bool spec, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
 {
-    if (spec) k_forward<M, MODE, true><<<grid, block, smem, st>>>(prm);
-    else k_forward<M, MODE, false><<<grid, block, 0, st>>>(prm);
+    if (spec) k_forward<M, MODE, SAMPLER, true><<<grid, block, smem, st>>>(prm);
+    else k_forward<M, MODE, SAMPLER, false><<<grid, block, 0, st>>>(prm);
     return cudaGetLastError();
 }
 
 template <int M>
-cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, bool spec, dim3 grid, dim3 block, size_t smem,
-                              cudaStream_t st)
+cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, bool spec, dim3 grid, dim3 block,
+                              size_t smem, cudaStream_t st)
 {
+    const bool lay = sampler == SAMPLER_LAYERED;
     switch (interp) {
-        case INTERP_TRILINEAR: return fwd_dispatch_spec<M, INTERP_TRILINEAR>(prm, spec, grid, block, smem, st);
-        case INTERP_TEXEMU: return fwd_dispatch_spec<M, INTERP_TEXEMU>(prm, spec, grid, block, smem, st);
-        case INTERP_TEXTURE: return fwd_dispatch_spec<M, INTERP_TEXTURE>(prm, spec, grid, block, smem, st);
+        case INTERP_TRILINEAR:
+            return lay ? fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_LAYERED>(prm, spec, grid, block, smem, st)
+                       : fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
+        case INTERP_TEXEMU:
+            return lay ? fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED>(prm, spec, grid, block, smem, st)
+                       : fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
+        case INTERP_TEXTURE:
+            return fwd_dispatch_spec<M, INTERP_TEXTURE, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -338,8 +365,8 @@ dim3 march_grid(const MarchParams& prm, const LaunchShape& ls)
 
 }  // namespace
 
-cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, bool do_spectral, const LaunchShape& ls,
-                           cudaStream_t st)
+cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sampler, bool do_spectral,
+                           const LaunchShape& ls, cudaStream_t st)
 {
     MarchParams prm = prm_in;
     prm.views_per_cta = ls.views_per_cta;
@@ -347,10 +374,10 @@ cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, bool do
     const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
     switch (M) {
-        case 1: return fwd_dispatch_mode<1>(prm, interp, do_spectral, grid, block, smem, st);
-        case 2: return fwd_dispatch_mode<2>(prm, interp, do_spectral, grid, block, smem, st);
-        case 3: return fwd_dispatch_mode<3>(prm, interp, do_spectral, grid, block, smem, st);
-        case 4: return fwd_dispatch_mode<4>(prm, interp, do_spectral, grid, block, smem, st);
+        case 1: return fwd_dispatch_mode<1>(prm, interp, sampler, do_spectral, grid, block, smem, st);
+        case 2: return fwd_dispatch_mode<2>(prm, interp, sampler, do_spectral, grid, block, smem, st);
+        case 3: return fwd_dispatch_mode<3>(prm, interp, sampler, do_spectral, grid, block, smem, st);
+        case 4: return fwd_dispatch_mode<4>(prm, interp, sampler, do_spectral, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
 }

@@ -9,7 +9,8 @@ namespace ctfp {
 struct MarchParams {
     GeomParams g;
     const float* vol[kMaxM];          // material densities [nz][ny][nx]
-    cudaTextureObject_t tex[kMaxM];   // same volumes as textures (TEXTURE mode)
+    cudaTextureObject_t tex[kMaxM];   // same volumes as 3D textures (TEXTURE mode)
+    cudaTextureObject_t ltex[kMaxM];  // same volumes as layered 2D textures (SAMPLER_LAYERED)
     float* L;                         // [P][V][U][M] path integrals (out, may be null)
     const float* Lin;                 // [P][V][U][M] path integrals (in, epilogue/adjoint)
     float* I;                         // [P][V][U] (may be null)
@@ -29,9 +30,10 @@ struct LaunchShape {
     int tile_u = 32, tile_v = 8, views_per_cta = 1;
 };
 
-// Launchers; all return cudaGetLastError() of the launch.
-cudaError_t launch_forward(const MarchParams& prm, int M, int interp, bool do_spectral, const LaunchShape& ls,
-                           cudaStream_t st);
+// Launchers; all return cudaGetLastError() of the launch.  sampler selects
+// SAMPLER_GLOBAL or SAMPLER_LAYERED for the software interp modes.
+cudaError_t launch_forward(const MarchParams& prm, int M, int interp, int sampler, bool do_spectral,
+                           const LaunchShape& ls, cudaStream_t st);
 cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st);
 cudaError_t launch_backward(const MarchParams& prm, int M, int interp, bool from_gL, const LaunchShape& ls,
                             cudaStream_t st);

@@ -34,9 +34,11 @@ using namespace ctfp;
 
 namespace {
 
-// Layout of the scratch array: view trigonometry, then attenuation, then
-// spectrum.  CTFP_NOALLOC_SCRATCH_BYTES is the stated maximum size.
-constexpr size_t kTrigBytes = sizeof(double2) * CTFP_NOALLOC_MAX_VIEWS;
+// Layout of the scratch array: view trigonometry in FP64 and FP32, then
+// attenuation, then spectrum.  CTFP_NOALLOC_SCRATCH_BYTES is the stated
+// maximum size.
+constexpr size_t kTrigBytes = sizeof(double2) * CTFP_NOALLOC_MAX_VIEWS + sizeof(float2) * CTFP_NOALLOC_MAX_VIEWS;
+constexpr size_t kTrigfOffset = sizeof(double2) * CTFP_NOALLOC_MAX_VIEWS;
 constexpr size_t kMuBytes = sizeof(float) * CTFP_MAX_ENERGIES * CTFP_MAX_MATERIALS;
 constexpr size_t kSpecBytes = sizeof(float) * CTFP_MAX_ENERGIES;
 static_assert(kTrigBytes + kMuBytes + kSpecBytes <= CTFP_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds its size");
@@ -92,11 +94,16 @@ __global__ void __launch_bounds__(256) k_forward_noalloc(const NoallocParams q)
     float acc[M], cmp[M];
 #pragma unroll
     for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+    // the same sample positions as ctfp_forward: FP64 for TRILINEAR, the
+    // reference's FP32 coordinates for the texture-unit emulation
+    const RayRef32 r = ray_ref32(q.g, p, v, u);
     for (int i = s.i0; i < s.i1; i++) {
         const double t = (double)i;
-        const Corner c = corner_of<MODE>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+        const Corner c = MODE == INTERP_TRILINEAR
+                             ? corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az))
+                             : corner_tex(ref32_coords(q.g, r, i));
         float val[M];
-        gather_interp<M>(q.vol, q.g.nx, q.g.ny, q.g.nz, c, val);
+        gather_interp<M, MODE>(q.vol, q.g.nx, q.g.ny, q.g.nz, c, val);
 #pragma unroll
         for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
     }
@@ -207,15 +214,19 @@ extern "C" ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_ma
     // before cudaMemcpyAsync returns, so these vectors may go out of scope)
     const int64_t P = g->projNum, E = n_energies, M = n_materials;
     std::vector<double2> trig((size_t)P);
+    std::vector<float2> trigf((size_t)P);
     for (int64_t k = 0; k < P; k++) {
         const double a = (double)angle_of(g, info, k);
         trig[(size_t)k] = make_double2(std::cos(a), std::sin(a));
+        trigf[(size_t)k] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     cudaStream_t s = (cudaStream_t)stream;
     double2* d_trig = (double2*)scratch;
+    float2* d_trigf = (float2*)(scratch + kTrigfOffset);
     float* d_mu = (float*)(scratch + kTrigBytes);
     float* d_S = (float*)(scratch + kTrigBytes + kMuBytes);
     e = cudaMemcpyAsync(d_trig, trig.data(), sizeof(double2) * (size_t)P, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_trigf, trigf.data(), sizeof(float2) * (size_t)P, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_mu, mu, sizeof(float) * (size_t)(E * M), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_S, spectrum, sizeof(float) * (size_t)E, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return nfail(CTFP_CUDA_ERROR, std::string("ctfp_forward_noalloc tables: ") + cudaGetErrorString(e));
@@ -231,6 +242,7 @@ extern "C" ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_ma
     gp.pHalfX = info.pHalfX; gp.pHalfY = info.pHalfY; gp.pHalfZ = info.pHalfZ;
     gp.pSizeX = info.pSizeX; gp.pSizeY = info.pSizeY; gp.pSizeZ = info.pSizeZ;
     gp.trig = d_trig;
+    gp.trigf = d_trigf;
     for (int m = 0; m < M; m++) q.vol[m] = volumes[m];
     q.S = d_S;
     q.mu = d_mu;

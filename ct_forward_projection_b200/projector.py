@@ -112,6 +112,10 @@ class Projector:
         call("ctfp_plan_set_interp", self._h, INTERP[interp])
         self.interp = interp
 
+    def set_sampler(self, sampler: str) -> None:
+        """'global' (linear volumes through L1) or 'layered' (texture gathers)."""
+        call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED}[sampler])
+
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta)
 

@@ -81,6 +81,16 @@ typedef enum ctfp_interp {
     CTFP_INTERP_TEXTURE = 2
 } ctfp_interp;
 
+/* Where the software samplers (TRILINEAR, TEXEMU) read a sample's 8 corners. */
+typedef enum ctfp_sampler {
+    /* the caller's linear volumes through L1 (8 loads per corner set) */
+    CTFP_SAMPLER_GLOBAL = 1,
+    /* plan-owned layered 2D textures, one layer per z slice: two texture
+     * gathers (tld4) return the 8 corners; weights stay in software.  Default;
+     * needs pNumZ <= 2048. */
+    CTFP_SAMPLER_LAYERED = 2
+} ctfp_sampler;
+
 /* Grid transmission table layout for ctfp_set_spectral_tables. */
 typedef enum ctfp_grid_layout {
     CTFP_GRID_NONE = 0,   /* no anti-scatter grid: G = 1                 */
@@ -110,6 +120,7 @@ ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_
 ctfp_status ctfp_plan_destroy(ctfp_plan* plan);
 ctfp_status ctfp_plan_get_system_info(const ctfp_plan* plan, ctfp_system_info* out);
 ctfp_status ctfp_plan_set_interp(ctfp_plan* plan, int32_t interp);
+ctfp_status ctfp_plan_set_sampler(ctfp_plan* plan, int32_t sampler);
 /* Ray-tile shape of the march kernels: tile_u x tile_v pixels per CTA (a
  * multiple of 32 threads, at most 256) and views_per_cta views marched by each
  * CTA for its tile.  Set by the autotuner; defaults 32 x 8 x 1. */
@@ -211,7 +222,7 @@ ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float*
  * contents: calls whose work overlaps on the GPU (different streams or threads)
  * race on it and must be serialised by the caller. */
 #define CTFP_NOALLOC_MAX_VIEWS 8192
-#define CTFP_NOALLOC_SCRATCH_BYTES (136 * 1024)
+#define CTFP_NOALLOC_SCRATCH_BYTES (200 * 1024)
 ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_materials, int32_t interp, int32_t n_energies,
                                  const float* spectrum, const float* mu, const float* grid, int32_t grid_layout,
                                  const float* det_response, float I0Val, const float* const* volumes, float* I,

@@ -48,26 +48,30 @@ GEOMS = [
 ]
 
 
+@pytest.mark.parametrize("sampler", ["layered", "global"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 3, 4])
-def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M):
+def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
     d = small_geometry(**GEOMS[gi])
     vols = random_volumes(d, M, 100 + gi * 7 + M)
     with Projector(d, M, "trilinear") as pr:
+        pr.set_sampler(sampler)
         L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1, M)
     Lref = O.line_integrals(d, vols, O.TRILINEAR)
     assert rel_err_scaled(L, Lref) < RTOL_TRI
 
 
+@pytest.mark.parametrize("sampler", ["layered", "global"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 4])
-def test_forward_trilinear_vs_oracle(cuda_ok, gi, M):
+def test_forward_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
     d = small_geometry(**GEOMS[gi])
     vols = random_volumes(d, M, 200 + gi + M)
     S, mu, G, D = spectral_setup(d, M, 17, 5 + gi)
     W = O.energy_weights(d, S, G, 2, D, 60000.0)
     ref = O.forward(d, vols, mu, W, O.TRILINEAR)
     with Projector(d, M, "trilinear") as pr:
+        pr.set_sampler(sampler)
         pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
         out = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
@@ -98,14 +102,16 @@ def test_forward_grid_layouts_and_no_response(cuda_ok, layout):
     assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TRI
 
 
+@pytest.mark.parametrize("sampler", ["layered", "global"])
 @pytest.mark.parametrize("M", [1, 2, 3])
-def test_forward_texemu_vs_oracle(cuda_ok, M):
+def test_forward_texemu_vs_oracle(cuda_ok, M, sampler):
     d = small_geometry(n=20, views=5, U=24, V=14)
     vols = random_volumes(d, M, 300 + M)
     S, mu, G, D = spectral_setup(d, M, 11, 9)
     W = O.energy_weights(d, S, G, 2, D, 60000.0)
     ref = O.forward(d, vols, mu, W, O.TEXEMU)
     with Projector(d, M, "texemu") as pr:
+        pr.set_sampler(sampler)
         pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
         out = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
@@ -139,8 +145,9 @@ def test_texture_weight_rounding_pinned(cuda_ok):
     hw = sample_volume(vol, pts_d, "texture").cpu().numpy()
     em = sample_volume(vol, pts_d, "texemu").cpu().numpy()
     tri = sample_volume(vol, pts_d, "trilinear").cpu().numpy()
-    assert np.max(np.abs(hw - em)) < 2e-5
-    assert np.max(np.abs(hw - tri)) < 8e-3
+    # same 8 corner weights; only the FP32 summation order of the unit differs
+    assert np.max(np.abs(hw - em)) < 1e-6
+    assert np.max(np.abs(hw - tri)) < 2e-2
 
 
 def test_zero_volume_is_flat_field(cuda_ok):

