@@ -41,6 +41,8 @@ struct ctfp_plan {
     cudaTextureObject_t ltex[kMaxM] = {};
     LaunchShape shape{};
     unsigned long long* d_count = nullptr;
+    // corner-expanded adjoint accumulators (allocated on first backward)
+    float4* d_gexp[kMaxM] = {};
     // staging for ctfp_forward_host
     float* h2d_vol[kMaxM] = {};
     float* d2h_I = nullptr;
@@ -247,6 +249,18 @@ MarchParams base_params(const ctfp_plan* p)
     return prm;
 }
 
+// Zeroed corner-expanded accumulators for one adjoint launch.
+ctfp_status prepare_expanded(ctfp_plan* p, MarchParams& prm, cudaStream_t st)
+{
+    const size_t n = expanded_elems(p->gp);
+    for (int m = 0; m < p->M; m++) {
+        if (!p->d_gexp[m]) CTFP_CUDA(cudaMalloc(&p->d_gexp[m], n * sizeof(float4)));
+        CTFP_CUDA(cudaMemsetAsync(p->d_gexp[m], 0, n * sizeof(float4), st));
+        prm.gexp[m] = p->d_gexp[m];
+    }
+    return CTFP_OK;
+}
+
 ctfp_status check_volumes(const ctfp_plan* p, const float* const* volumes)
 {
     if (!volumes) return fail(CTFP_INVALID_ARG, "volumes is NULL");
@@ -366,6 +380,7 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     cudaFree(p->d_I0);
     cudaFree(p->d_count);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
+    for (int m = 0; m < kMaxM; m++) cudaFree(p->d_gexp[m]);
     cudaFree(p->d2h_I);
     cudaFree(p->d2h_IAbs);
     delete p;
@@ -554,7 +569,11 @@ ctfp_status ctfp_backward(ctfp_plan* p, const float* L_ckpt, const float* gI, co
     prm.gI = gI;
     prm.gIAbs = gIAbsorb;
     for (int m = 0; m < p->M; m++) prm.gvol[m] = g_volumes[m];
-    CTFP_CUDA(launch_backward(prm, p->M, p->interp, false, p->shape, (cudaStream_t)stream));
+    cudaStream_t s = (cudaStream_t)stream;
+    ctfp_status st = prepare_expanded(p, prm, s);
+    if (st != CTFP_OK) return st;
+    CTFP_CUDA(launch_backward(prm, p->M, p->interp, false, p->shape, s));
+    CTFP_CUDA(launch_fold(prm, p->M, s));
     return CTFP_OK;
 }
 
@@ -567,7 +586,11 @@ ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* p, const float* gL, float* co
     MarchParams prm = base_params(p);
     prm.Lin = gL;
     for (int m = 0; m < p->M; m++) prm.gvol[m] = g_volumes[m];
-    CTFP_CUDA(launch_backward(prm, p->M, p->interp, true, p->shape, (cudaStream_t)stream));
+    cudaStream_t s = (cudaStream_t)stream;
+    ctfp_status st = prepare_expanded(p, prm, s);
+    if (st != CTFP_OK) return st;
+    CTFP_CUDA(launch_backward(prm, p->M, p->interp, true, p->shape, s));
+    CTFP_CUDA(launch_fold(prm, p->M, s));
     return CTFP_OK;
 }
 
@@ -646,13 +669,18 @@ const float* plan_W(const ctfp_plan* p) { return p->d_W; }
 LaunchShape& plan_shape(ctfp_plan* p) { return p->shape; }
 }  // namespace ctfp
 
-extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, int32_t tile_v, int32_t views_per_cta)
+extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,
+                                                  int32_t min_ctas_per_sm)
 {
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
     if (tile_u < 1 || tile_v < 1 || tile_u * tile_v > 256 || (tile_u * tile_v) % 32 != 0 || views_per_cta < 1)
         return fail(CTFP_INVALID_ARG, "tile_u*tile_v must be a multiple of 32 and at most 256");
+    if (min_ctas_per_sm < 2 || min_ctas_per_sm > 4) return fail(CTFP_INVALID_ARG, "min_ctas_per_sm must be 2, 3 or 4");
+    if (tile_u * tile_v * min_ctas_per_sm > 2048)
+        return fail(CTFP_INVALID_ARG, "tile_u*tile_v*min_ctas_per_sm exceeds 2048 threads per SM");
     p->shape.tile_u = tile_u;
     p->shape.tile_v = tile_v;
     p->shape.views_per_cta = views_per_cta;
+    p->shape.min_ctas = min_ctas_per_sm;
     return CTFP_OK;
 }

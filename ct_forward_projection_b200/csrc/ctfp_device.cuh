@@ -152,6 +152,7 @@ __device__ __forceinline__ float3 ref32_coords(const GeomParams& g, const RayRef
 // relative accuracy (1 - w computed from a rounded w near 1 would not).
 struct Corner {
     int ix, iy, iz;
+    float tx, ty;    // ix + 1, iy + 1 as FP32: the gather coordinate of the layered sampler
     float wx, wy, wz;
     float ux, uy, uz;
     int qx, qy, qz;  // TEXEMU: the texture unit's 8-bit fractions (0..255)
@@ -205,12 +206,26 @@ __device__ __forceinline__ float interp8(const Corner& c, const float* v)
 // x * 256 - 127.5 is exact in FP32 for |x| < 2^15.
 __device__ __forceinline__ int tex_fixed(float x) { return (int)floorf(fmaf(x, 256.0f, -127.5f)); }
 
+// The two weights of one axis from the exact FP64 fraction f in [0, 1): the
+// smaller of f and 1 - f (both exact in FP64) is rounded once to FP32 and the
+// larger is formed from it in FP32, which is accurate in absolute terms and
+// so relative to a value >= 1/2.  One conversion per axis.
+__device__ __forceinline__ void frac_pair(double f, float& w, float& u)
+{
+    const bool lo = f < 0.5;
+    const float sm = (float)(lo ? f : 1.0 - f);
+    const float bg = 1.0f - sm;
+    w = lo ? sm : bg;
+    u = lo ? bg : sm;
+}
+
 // Texture-unit footprint at the FP32 tex3D coordinate (x, y, z) = index + 0.5.
 __device__ __forceinline__ Corner corner_tex(float3 x)
 {
     Corner c = {};
     const int X = tex_fixed(x.x), Y = tex_fixed(x.y), Z = tex_fixed(x.z);
     c.ix = X >> 8; c.iy = Y >> 8; c.iz = Z >> 8;
+    c.tx = (float)(c.ix + 1); c.ty = (float)(c.iy + 1);
     c.qx = X & 255; c.qy = Y & 255; c.qz = Z & 255;
     return c;
 }
@@ -225,8 +240,10 @@ __device__ __forceinline__ Corner corner_of(double cx, double cy, double cz)
     if (MODE == INTERP_TRILINEAR) {
         const double fx = floor(cx), fy = floor(cy), fz = floor(cz);
         c.ix = (int)fx; c.iy = (int)fy; c.iz = (int)fz;
-        c.wx = (float)(cx - fx); c.wy = (float)(cy - fy); c.wz = (float)(cz - fz);
-        c.ux = (float)((fx + 1.0) - cx); c.uy = (float)((fy + 1.0) - cy); c.uz = (float)((fz + 1.0) - cz);
+        c.tx = (float)(fx + 1.0); c.ty = (float)(fy + 1.0);
+        frac_pair(cx - fx, c.wx, c.ux);
+        frac_pair(cy - fy, c.wy, c.uy);
+        frac_pair(cz - fz, c.wz, c.uz);
     } else {
         const int X = tex_fixed((float)(cx + 0.5)), Y = tex_fixed((float)(cy + 0.5)), Z = tex_fixed((float)(cz + 0.5));
         c.ix = X >> 8; c.iy = Y >> 8; c.iz = Z >> 8;
@@ -276,14 +293,13 @@ __device__ __forceinline__ void gather_interp(const float* const* __restrict__ v
 
 // Four texels of the 2x2 footprint with lower corner (ix, iy) in one layer
 // of a layered 2D texture (tld4, PTX "texture gather").  The coordinate is the
-// footprint's centre, ix + 1 (x_B = ix + 0.5), so the unit's own 8-bit
-// coordinate rounding cannot move the footprint.  Returned in gather order:
+// footprint's centre, (x, y) = (ix + 1, iy + 1) (x_B = ix + 0.5), so the unit's
+// own 8-bit coordinate rounding cannot move the footprint.  Returned in gather order:
 // x = (ix, iy+1), y = (ix+1, iy+1), z = (ix+1, iy), w = (ix, iy).  Border
 // addressing reads 0 outside the layer.
-__device__ __forceinline__ float4 gather_layer(cudaTextureObject_t t, int layer, int ix, int iy)
+__device__ __forceinline__ float4 gather_layer(cudaTextureObject_t t, int layer, float x, float y)
 {
     float4 r;
-    const float x = (float)ix + 1.0f, y = (float)iy + 1.0f;
     asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
         : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
         : "l"(t), "r"(layer), "f"(x), "f"(y), "f"(y));
@@ -300,8 +316,8 @@ __device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, 
     const int l0 = z0ok ? c.iz : 0, l1 = z1ok ? c.iz + 1 : 0;
 #pragma unroll
     for (int m = 0; m < M; m++) {
-        float4 a = gather_layer(ltex[m], l0, c.ix, c.iy);
-        float4 b = gather_layer(ltex[m], l1, c.ix, c.iy);
+        float4 a = gather_layer(ltex[m], l0, c.tx, c.ty);
+        float4 b = gather_layer(ltex[m], l1, c.tx, c.ty);
         if (!z0ok) a = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!z1ok) b = make_float4(0.f, 0.f, 0.f, 0.f);
         const float v[8] = {a.w, a.z, a.x, a.y, b.w, b.z, b.x, b.y};
@@ -309,14 +325,30 @@ __device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, 
     }
 }
 
-// Scatters w_k * g[m] into the 8 corners of M gradient volumes (the
-// transposed interpolation weights), skipping corners outside the volume.
-template <int M, int MODE>
-__device__ __forceinline__ void scatter_interp(float* const* __restrict__ gvol, int nx, int ny, int nz,
-                                               const Corner& c, const float* g)
+// Corner-expanded adjoint accumulator.  The 8 transposed weights of a sample
+// go to two float4 cells, one per z slice of the footprint: cell (z, y, x)
+// holds the contributions of footprints with lower corner (x, y) in slice z to
+// the 4 voxels (x, y), (x+1, y), (x, y+1), (x+1, y+1).  Two 16-byte vector
+// reductions replace 8 scalar atomics; k_fold later sums the 4 cells that
+// touch each voxel.  Indices are offset by one in x and y and by one in z so
+// that footprints hanging over the volume's edge land in padding.
+__device__ __forceinline__ size_t exp_index(int nx, int ny, int x, int y, int z)
 {
-    const int nxy = nx * ny;
-    const int base = (c.iz * ny + c.iy) * nx + c.ix;
+    return ((size_t)(z + 1) * (size_t)(ny + 1) + (size_t)(y + 1)) * (size_t)(nx + 1) + (size_t)(x + 1);
+}
+
+__device__ __forceinline__ void red_add_v4(float4* p, float a, float b, float c, float d)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+template <int M, int MODE>
+__device__ __forceinline__ void scatter_expanded(float4* const* __restrict__ gexp, int nx, int ny, int nz,
+                                                 const Corner& c, const float* g)
+{
+    // footprints lie within [-1, n] on every axis: the clipped sample range
+    // only holds samples whose footprint touches the volume
     float w[8];
     if (MODE == 1 /* INTERP_TEXEMU */) {
         texunit_weights(c.qx, c.qy, c.qz, w);
@@ -325,14 +357,13 @@ __device__ __forceinline__ void scatter_interp(float* const* __restrict__ gvol, 
         w[0] = ux * uy * uz; w[1] = c.wx * uy * uz; w[2] = ux * c.wy * uz; w[3] = c.wx * c.wy * uz;
         w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
     }
-    const int off[8] = {0, 1, nx, nx + 1, nxy, nxy + 1, nxy + nx, nxy + nx + 1};
+    if (c.ix < -1 || c.iy < -1 || c.iz < -1 || c.ix >= nx || c.iy >= ny || c.iz >= nz) return;
+    const size_t i0 = exp_index(nx, ny, c.ix, c.iy, c.iz);
+    const size_t i1 = exp_index(nx, ny, c.ix, c.iy, c.iz + 1);
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int x = c.ix + (k & 1), y = c.iy + ((k >> 1) & 1), z = c.iz + ((k >> 2) & 1);
-        if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
-#pragma unroll
-            for (int m = 0; m < M; m++) atomicAdd(gvol[m] + base + off[k], w[k] * g[m]);
-        }
+    for (int m = 0; m < M; m++) {
+        red_add_v4(gexp[m] + i0, w[0] * g[m], w[1] * g[m], w[2] * g[m], w[3] * g[m]);
+        red_add_v4(gexp[m] + i1, w[4] * g[m], w[5] * g[m], w[6] * g[m], w[7] * g[m]);
     }
 }
 

@@ -132,8 +132,8 @@ __device__ __forceinline__ void load_L(const float* L, int64_t ray, float* l)
 }
 
 // K1+K2. Grid: x = pixel tiles along u, y = along v, z = view groups.
-template <int M, int MODE, int SAMPLER, bool SPECTRAL>
-__global__ void __launch_bounds__(256) k_forward(const MarchParams prm)
+template <int M, int MODE, int SAMPLER, bool SPECTRAL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_forward(const MarchParams prm)
 {
     extern __shared__ float s_mu[];
     if (SPECTRAL) load_mu(s_mu, prm.mu, prm.E * M);
@@ -227,14 +227,34 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
             for (int i = s.i0; i < s.i1; i++) {
                 const double t = (double)i;
                 const Corner c = corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
-                scatter_interp<M, INTERP_TRILINEAR>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
+                scatter_expanded<M, INTERP_TRILINEAR>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
             }
         } else {
             // transpose of the texture-unit sampler at the reference's FP32 coordinates
             const RayRef32 r = ray_ref32(prm.g, p, v, u);
             for (int i = s.i0; i < s.i1; i++)
-                scatter_interp<M, INTERP_TEXEMU>(prm.gvol, prm.g.nx, prm.g.ny, prm.g.nz,
-                                                 corner_tex(ref32_coords(prm.g, r, i)), g);
+                scatter_expanded<M, INTERP_TEXEMU>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz,
+                                                   corner_tex(ref32_coords(prm.g, r, i)), g);
+        }
+    }
+}
+
+// Sums the corner-expanded accumulators into the gradient volumes:
+// g[z][y][x] += cell(z, y, x).x + cell(z, y, x-1).y + cell(z, y-1, x).z +
+// cell(z, y-1, x-1).w.  One streaming pass.
+template <int M>
+__global__ void k_fold(const MarchParams prm)
+{
+    const int nx = prm.g.nx, ny = prm.g.ny, nz = prm.g.nz;
+    const int64_t n = (int64_t)nx * ny * nz;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((int64_t)nx * ny));
+        const size_t a = exp_index(nx, ny, x, y, z), b = exp_index(nx, ny, x - 1, y, z);
+        const size_t c = exp_index(nx, ny, x, y - 1, z), d = exp_index(nx, ny, x - 1, y - 1, z);
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            const float4* e = prm.gexp[m];
+            prm.gvol[m][k] += (e[a].x + e[b].y) + (e[c].z + e[d].w);
         }
     }
 }
@@ -316,28 +336,39 @@ __global__ void k_count_support(const GeomParams g, unsigned long long* out)
     if ((threadIdx.x & 31) == 0) atomicAdd(out, n);
 }
 
-template <int M, int MODE, int SAMPLER>
-cudaError_t fwd_dispatch_spec(const MarchParams& prm, bool spec, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+template <int M, int MODE, int SAMPLER, int MINB>
+cudaError_t fwd_launch(const MarchParams& prm, bool spec, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
 {
-    if (spec) k_forward<M, MODE, SAMPLER, true><<<grid, block, smem, st>>>(prm);
-    else k_forward<M, MODE, SAMPLER, false><<<grid, block, 0, st>>>(prm);
+    if (spec) k_forward<M, MODE, SAMPLER, true, MINB><<<grid, block, smem, st>>>(prm);
+    else k_forward<M, MODE, SAMPLER, false, MINB><<<grid, block, 0, st>>>(prm);
     return cudaGetLastError();
 }
 
+template <int M, int MODE, int SAMPLER>
+cudaError_t fwd_dispatch_spec(const MarchParams& prm, bool spec, int minb, dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st)
+{
+    switch (minb) {
+        case 3: return fwd_launch<M, MODE, SAMPLER, 3>(prm, spec, grid, block, smem, st);
+        case 4: return fwd_launch<M, MODE, SAMPLER, 4>(prm, spec, grid, block, smem, st);
+        default: return fwd_launch<M, MODE, SAMPLER, 2>(prm, spec, grid, block, smem, st);
+    }
+}
+
 template <int M>
-cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, bool spec, dim3 grid, dim3 block,
-                              size_t smem, cudaStream_t st)
+cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, bool spec, int minb, dim3 grid,
+                              dim3 block, size_t smem, cudaStream_t st)
 {
     const bool lay = sampler == SAMPLER_LAYERED;
     switch (interp) {
         case INTERP_TRILINEAR:
-            return lay ? fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_LAYERED>(prm, spec, grid, block, smem, st)
-                       : fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
+            return lay ? fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_LAYERED>(prm, spec, minb, grid, block, smem, st)
+                       : fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
         case INTERP_TEXEMU:
-            return lay ? fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED>(prm, spec, grid, block, smem, st)
-                       : fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
+            return lay ? fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED>(prm, spec, minb, grid, block, smem, st)
+                       : fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
         case INTERP_TEXTURE:
-            return fwd_dispatch_spec<M, INTERP_TEXTURE, SAMPLER_GLOBAL>(prm, spec, grid, block, smem, st);
+            return fwd_dispatch_spec<M, INTERP_TEXTURE, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -374,10 +405,10 @@ cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sam
     const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
     switch (M) {
-        case 1: return fwd_dispatch_mode<1>(prm, interp, sampler, do_spectral, grid, block, smem, st);
-        case 2: return fwd_dispatch_mode<2>(prm, interp, sampler, do_spectral, grid, block, smem, st);
-        case 3: return fwd_dispatch_mode<3>(prm, interp, sampler, do_spectral, grid, block, smem, st);
-        case 4: return fwd_dispatch_mode<4>(prm, interp, sampler, do_spectral, grid, block, smem, st);
+        case 1: return fwd_dispatch_mode<1>(prm, interp, sampler, do_spectral, ls.min_ctas, grid, block, smem, st);
+        case 2: return fwd_dispatch_mode<2>(prm, interp, sampler, do_spectral, ls.min_ctas, grid, block, smem, st);
+        case 3: return fwd_dispatch_mode<3>(prm, interp, sampler, do_spectral, ls.min_ctas, grid, block, smem, st);
+        case 4: return fwd_dispatch_mode<4>(prm, interp, sampler, do_spectral, ls.min_ctas, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -415,6 +446,23 @@ cudaError_t launch_backward(const MarchParams& prm_in, int M, int interp, bool f
         case 4: return bwd_dispatch<4>(prm, interp, from_gL, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
+}
+
+size_t expanded_elems(const GeomParams& g) { return (size_t)(g.nz + 2) * (size_t)(g.ny + 1) * (size_t)(g.nx + 1); }
+
+cudaError_t launch_fold(const MarchParams& prm, int M, cudaStream_t st)
+{
+    const int64_t n = (int64_t)prm.g.nx * prm.g.ny * prm.g.nz;
+    int64_t nb = (n + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    switch (M) {
+        case 1: k_fold<1><<<(unsigned)nb, 256, 0, st>>>(prm); break;
+        case 2: k_fold<2><<<(unsigned)nb, 256, 0, st>>>(prm); break;
+        case 3: k_fold<3><<<(unsigned)nb, 256, 0, st>>>(prm); break;
+        case 4: k_fold<4><<<(unsigned)nb, 256, 0, st>>>(prm); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_weights(const float* spectrum, const float* grid, int grid_layout, const float* det, float I0Val,

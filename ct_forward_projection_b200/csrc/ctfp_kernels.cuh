@@ -20,6 +20,7 @@ struct MarchParams {
     const float* gI;                  // [P][V][U] dLoss/dI (adjoint)
     const float* gIAbs;               // [P][V][U] dLoss/dIAbsorb (adjoint, may be null)
     float* gvol[kMaxM];               // gradient volumes (adjoint)
+    float4* gexp[kMaxM];              // corner-expanded gradient accumulators (adjoint), see k_fold
     int E;
     int view0;                        // first view of this launch
     int n_views;                      // views in this launch
@@ -27,7 +28,8 @@ struct MarchParams {
 };
 
 struct LaunchShape {
-    int tile_u = 32, tile_v = 8, views_per_cta = 1;
+    int tile_u = 16, tile_v = 8, views_per_cta = 2;
+    int min_ctas = 4;  // register cap of the forward march: 65536 / (256 * min_ctas) per thread
 };
 
 // Launchers; all return cudaGetLastError() of the launch.  sampler selects
@@ -35,8 +37,13 @@ struct LaunchShape {
 cudaError_t launch_forward(const MarchParams& prm, int M, int interp, int sampler, bool do_spectral,
                            const LaunchShape& ls, cudaStream_t st);
 cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st);
+// Adjoint scatter into the corner-expanded accumulators prm.gexp (zeroed by
+// the caller), followed by launch_fold into prm.gvol.
 cudaError_t launch_backward(const MarchParams& prm, int M, int interp, bool from_gL, const LaunchShape& ls,
                             cudaStream_t st);
+cudaError_t launch_fold(const MarchParams& prm, int M, cudaStream_t st);
+// Elements of one corner-expanded accumulator: (nz + 2) x (ny + 1) x (nx + 1) float4.
+size_t expanded_elems(const GeomParams& g);
 cudaError_t launch_weights(const float* spectrum, const float* grid, int grid_layout, const float* det,
                            float I0Val, int E, int U, int V, float* W, float* I0, cudaStream_t st);
 cudaError_t launch_finalize(int64_t n_pix, int64_t n_views, const float* I, const float* IAbs, const float* I0,

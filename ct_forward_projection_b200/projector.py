@@ -116,8 +116,8 @@ class Projector:
         """'global' (linear volumes through L1) or 'layered' (texture gathers)."""
         call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED}[sampler])
 
-    def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1) -> None:
-        call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta)
+    def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
+        call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)
 
     # -- tables -------------------------------------------------------------
     def set_spectral_tables(self, spectrum, mu, grid=None, grid_layout: int | None = None, det_response=None,

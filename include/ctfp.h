@@ -122,9 +122,12 @@ ctfp_status ctfp_plan_get_system_info(const ctfp_plan* plan, ctfp_system_info* o
 ctfp_status ctfp_plan_set_interp(ctfp_plan* plan, int32_t interp);
 ctfp_status ctfp_plan_set_sampler(ctfp_plan* plan, int32_t sampler);
 /* Ray-tile shape of the march kernels: tile_u x tile_v pixels per CTA (a
- * multiple of 32 threads, at most 256) and views_per_cta views marched by each
- * CTA for its tile.  Set by the autotuner; defaults 32 x 8 x 1. */
-ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t tile_v, int32_t views_per_cta);
+ * multiple of 32 threads, at most 256), views_per_cta views marched by each
+ * CTA for its tile, and min_ctas_per_sm (2, 3 or 4), the residency the forward
+ * march is compiled for (its register cap: 65536 / (256 * min_ctas_per_sm)).
+ * Set by the autotuner; defaults 16 x 8 x 2 x 4. */
+ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,
+                                       int32_t min_ctas_per_sm);
 
 /* Spectral tables, host pointers, copied into the plan.
  *   spectrum     [E]     normalised spectrum S_e
