@@ -72,13 +72,15 @@ def build_compat(force: bool = False) -> str | None:
     if not os.path.isdir(COMPAT):
         return None
     srcs = sorted(os.path.join(COMPAT, f) for f in os.listdir(COMPAT) if f.endswith(".cpp"))
+    srcs += [os.path.join(COMPAT, "ini", "InitFile.cpp")]
     if not srcs:
         return None
-    deps = _deps(COMPAT, (".cpp", ".h")) + [LIB]
+    deps = _deps(COMPAT, (".cpp", ".h")) + _deps(os.path.join(COMPAT, "ini"), (".cpp", ".h")) + [LIB]
     if not force and _newer(COMPAT_LIB, deps) and _newer(CLI, deps):
         return COMPAT_LIB
     lib_srcs = [s for s in srcs if not s.endswith("main.cpp")]
-    cflags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", INCLUDE, "-I", COMPAT]
+    cflags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", INCLUDE, "-I", COMPAT, "-I",
+              os.path.join(COMPAT, "ini"), "-I", "/usr/local/cuda/include"]
     _run(["g++", *cflags, "-shared", "-o", COMPAT_LIB, *lib_srcs, "-L", PKG, "-lctfp",
           "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart"])
     main = [s for s in srcs if s.endswith("main.cpp")]
