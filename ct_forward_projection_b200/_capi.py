@@ -44,6 +44,12 @@ class SystemInfo(C.Structure):
                [("intNum", C.c_int64)]
 
 
+class LaunchShape(C.Structure):
+    """ctfp_launch_shape — the autotuner's choice."""
+    _fields_ = [("tile_u", C.c_int32), ("tile_v", C.c_int32), ("views_per_cta", C.c_int32),
+                ("min_ctas_per_sm", C.c_int32), ("ms", C.c_float), ("from_cache", C.c_int32)]
+
+
 class GridParams(C.Structure):
     """ctfp_grid_params — GridInfo geometry (DataType.h:57-75)."""
     _fields_ = [("gridStripsWidth", C.c_int32), ("interspaceWidth", C.c_int32), ("h", C.c_float),
@@ -80,6 +86,12 @@ _SIGNATURES = {
     "ctfp_labels_to_density": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, _P]),
     "ctfp_forward_noalloc": (C.c_int, [C.POINTER(Geometry), C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
                                        _P, C.c_float, _P, _P, _P, _P, _P]),
+    "ctfp_plan_autotune": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.POINTER(LaunchShape), _P]),
+    "ctfp_batch_create": (C.c_int, [C.c_int32, _P, C.POINTER(_P)]),
+    "ctfp_batch_destroy": (C.c_int, [_P]),
+    "ctfp_batch_forward": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "ctfp_batch_forward_adjoint": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "ctfp_batch_info": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ctfp_last_error_string": (C.c_char_p, []),
     "ctfp_version": (C.c_char_p, []),
 }

@@ -667,6 +667,16 @@ int plan_energies(const ctfp_plan* p) { return p->spectral_ready ? p->E : 0; }
 const float* plan_mu(const ctfp_plan* p) { return p->d_mu; }
 const float* plan_W(const ctfp_plan* p) { return p->d_W; }
 LaunchShape& plan_shape(ctfp_plan* p) { return p->shape; }
+cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m) { return p->ltex[m]; }
+MarchParams plan_march_params(const ctfp_plan* p) { return base_params(p); }
+const ctfp_geometry& plan_geometry(const ctfp_plan* p) { return p->geom; }
+// Copies the caller's volumes into the plan's layered arrays on stream st.
+ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
+{
+    ctfp_status s = check_volumes(p, volumes);
+    if (s != CTFP_OK) return s;
+    return upload_textures(p, volumes, st);
+}
 }  // namespace ctfp
 
 extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,

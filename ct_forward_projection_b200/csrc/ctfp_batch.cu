@@ -1,0 +1,574 @@
+// ctfp_batch.cu — the batched form: many independent problems (their own
+// geometry, materials, spectra, view counts) in one persistent launch over a
+// work queue, replayed as a CUDA graph.  No reference counterpart.
+//
+// Work unit = (item, view, 16 x 8 pixel tile).  The persistent grid is sized
+// to the device's residency; each CTA takes units from a global counter
+// (atomicAdd, no waits), items ordered by estimated cost, largest first, so
+// the long problems start early and the short ones fill the tail.
+//
+// Two kernels run per batch: the forward (march + spectral epilogue, optional
+// checkpoint), and the fused forward + loss + adjoint, which for every ray
+// marches, forms I, the loss sum (log I - log I_target)^2 and its gradient,
+// the spectral-weight recompute, and the adjoint march scattering into the
+// corner-expanded accumulators (two 16-byte vector reductions per sample and
+// material); a fold kernel then adds the accumulators into the gradients.
+#include <algorithm>
+#include <new>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/ctfp.h"
+#include "ctfp_kernels.cuh"
+
+namespace ctfp {
+void set_last_error(const std::string& msg);
+const GeomParams& plan_geom(const ctfp_plan* p);
+int plan_materials(const ctfp_plan* p);
+int plan_interp(const ctfp_plan* p);
+int plan_sampler(const ctfp_plan* p);
+int plan_device(const ctfp_plan* p);
+int plan_energies(const ctfp_plan* p);
+const float* plan_mu(const ctfp_plan* p);
+const float* plan_W(const ctfp_plan* p);
+cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m);
+ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t st);
+}  // namespace ctfp
+
+using namespace ctfp;
+
+namespace {
+
+constexpr int kTU = 16, kTV = 8, kThreads = kTU * kTV;
+
+// One item as the persistent kernels see it.  The pointer fields are refreshed
+// per call from the batch's staging table.
+struct ItemDesc {
+    GeomParams g;
+    cudaTextureObject_t ltex[kMaxM];
+    const float* mu;   // [E][M]
+    const float* W;    // [E][V][U]
+    int M, E, interp;
+    int tiles_u, tiles_v;
+    long long unit0;   // first global unit of this item
+    long long units;
+    // per call
+    float* I;
+    float* IAbs;
+    float* L;
+    const float* I_target;
+    float* gvol[kMaxM];
+    float4* gexp[kMaxM];
+    float* loss;       // device scalar accumulated with atomicAdd
+};
+
+struct BatchArgs {
+    const ItemDesc* items;
+    int n_items;
+    long long total_units;
+    unsigned long long* counter;
+};
+
+__device__ __forceinline__ int find_item(const BatchArgs& a, long long unit)
+{
+    int lo = 0, hi = a.n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.items[mid].unit0 <= unit) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ long long next_unit(const BatchArgs& a, long long* s_unit)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) *s_unit = (long long)atomicAdd(a.counter, 1ull);
+    __syncthreads();
+    return *s_unit;
+}
+
+// Path integrals of one ray through the layered sampler.
+template <int M, int MODE>
+__device__ __forceinline__ void batch_march(const ItemDesc& it, int p, int v, int u, float* L)
+{
+    const RaySeg s = ray_segment(it.g, p, v, u);
+    float acc[M], cmp[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+    const RayRef32 r = ray_ref32(it.g, p, v, u);
+    for (int i = s.i0; i < s.i1; i++) {
+        const double t = (double)i;
+        const Corner c = MODE == INTERP_TRILINEAR
+                             ? corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az))
+                             : corner_tex(ref32_coords(it.g, r, i));
+        float val[M];
+        gather4_interp<M, MODE>(it.ltex, it.g.nz, c, val);
+#pragma unroll
+        for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) L[m] = it.g.dx * (acc[m] - cmp[m]);
+}
+
+template <int M, int MODE>
+__device__ __forceinline__ void batch_scatter(const ItemDesc& it, int p, int v, int u, const float* g)
+{
+    const RaySeg s = ray_segment(it.g, p, v, u);
+    const RayRef32 r = ray_ref32(it.g, p, v, u);
+    for (int i = s.i0; i < s.i1; i++) {
+        const double t = (double)i;
+        const Corner c = MODE == INTERP_TRILINEAR
+                             ? corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az))
+                             : corner_tex(ref32_coords(it.g, r, i));
+        scatter_expanded<M, MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(it.gexp, it.g.nx, it.g.ny,
+                                                                                         it.g.nz, c, g);
+    }
+}
+
+// One ray of one unit.  ADJOINT: the fused forward + loss + adjoint.
+template <int M, int MODE, bool ADJOINT>
+__device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_mu, int p, int v, int u)
+{
+    const int64_t npix = (int64_t)it.g.U * it.g.V;
+    const int64_t pix = (int64_t)v * it.g.U + u;
+    const int64_t ray = (int64_t)p * npix + pix;
+    float L[M];
+    batch_march<M, MODE>(it, p, v, u, L);
+    float sI = 0.f, cI = 0.f, sA = 0.f, cA = 0.f, S[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) S[m] = 0.f;
+    for (int e = 0; e < it.E; e++) {
+        float att = 0.f;
+#pragma unroll
+        for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
+        const float w = __ldg(it.W + (int64_t)e * npix + pix);
+        float ex, om;
+        if (att < 0.25f) {
+            om = -expm1f(-att);
+            ex = 1.0f - om;
+        } else {
+            ex = expf(-att);
+            om = 1.0f - ex;
+        }
+        const float Ie = w * ex;
+        kahan_add(sI, cI, Ie);
+        kahan_add(sA, cA, w * om);
+        if (ADJOINT) {
+#pragma unroll
+            for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
+        }
+    }
+    const float I = sI - cI;
+    if (it.I) it.I[ray] = I;
+    if (it.IAbs) it.IAbs[ray] = sA - cA;
+    if (it.L) {
+#pragma unroll
+        for (int m = 0; m < M; m++) it.L[ray * M + m] = L[m];
+    }
+    if (!ADJOINT) return 0.f;
+    // loss (log I - log I_t)^2 and dLoss/dI = 2 (log I - log I_t) / I; dI/dL_m = -S_m
+    if (!(I > 0.f)) return 0.f;
+    const float res = logf(I) - logf(it.I_target[ray]);
+    const float gI = 2.0f * res / I;
+    float g[M];
+    bool any = false;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        g[m] = -gI * S[m] * it.g.dx;
+        any |= g[m] != 0.f;
+    }
+    if (any) batch_scatter<M, MODE>(it, p, v, u, g);
+    return res * res;
+}
+
+// Residency: forward 6 CTAs of 128 threads per SM (80 registers, no spill);
+// the fused adjoint 5 (the scatter needs more registers).
+template <bool ADJOINT>
+__global__ void __launch_bounds__(kThreads, ADJOINT ? 5 : 6) k_batch(const BatchArgs a)
+{
+    __shared__ float s_mu[CTFP_MAX_ENERGIES * kMaxM];
+    __shared__ long long s_unit;
+    __shared__ float s_loss[kThreads / 32];
+    int cached = -1;
+    for (;;) {
+        const long long unit = next_unit(a, &s_unit);
+        if (unit >= a.total_units) break;
+        const int k = find_item(a, unit);
+        const ItemDesc& it = a.items[k];
+        if (k != cached) {
+            for (int j = threadIdx.x; j < it.E * it.M; j += blockDim.x) s_mu[j] = it.mu[j];
+            cached = k;
+            __syncthreads();
+        }
+        const long long local = unit - it.unit0;
+        const int tiles = it.tiles_u * it.tiles_v;
+        const int p = (int)(local / tiles);
+        const int tile = (int)(local % tiles);
+        const int u = (tile % it.tiles_u) * kTU + (int)(threadIdx.x % kTU);
+        const int v = (tile / it.tiles_u) * kTV + (int)(threadIdx.x / kTU);
+        float loss = 0.f;
+        if (u < it.g.U && v < it.g.V) {
+            const bool tri = it.interp == INTERP_TRILINEAR;
+            switch (it.M) {
+                case 1: loss = tri ? process_ray<1, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
+                                   : process_ray<1, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
+                case 2: loss = tri ? process_ray<2, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
+                                   : process_ray<2, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
+                case 3: loss = tri ? process_ray<3, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
+                                   : process_ray<3, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
+                default: loss = tri ? process_ray<4, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
+                                    : process_ray<4, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
+            }
+        }
+        if (ADJOINT && it.loss) {
+            for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
+            if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = loss;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float t = 0.f;
+                for (int w = 0; w < kThreads / 32; w++) t += s_loss[w];
+                atomicAdd(it.loss, t);
+            }
+        }
+    }
+}
+
+// Folds every item's corner-expanded accumulators into its gradients.
+__global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long* vox0, long long total)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (vox0[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const ItemDesc& it = items[lo];
+        const long long k = t - vox0[lo];
+        const int nx = it.g.nx, ny = it.g.ny;
+        const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((long long)nx * ny));
+        const size_t a = exp_index(nx, ny, x, y, z), b = exp_index(nx, ny, x - 1, y, z);
+        const size_t c = exp_index(nx, ny, x, y - 1, z), d = exp_index(nx, ny, x - 1, y - 1, z);
+        for (int m = 0; m < it.M; m++) {
+            const float4* e = it.gexp[m];
+            it.gvol[m][k] += (e[a].x + e[b].y) + (e[c].z + e[d].w);
+        }
+    }
+}
+
+}  // namespace
+
+struct ctfp_batch {
+    int n = 0;
+    int device = 0;
+    std::vector<ctfp_plan*> plans;
+    std::vector<int> order;            // item slots in cost order
+    std::vector<long long> vox0;       // first voxel of each slot in the fold's flat index
+    std::vector<ItemDesc> items;       // tables of the current call
+    ItemDesc* d_items[2] = {nullptr, nullptr};  // device tables of the forward, forward + adjoint graphs
+    long long* d_vox0 = nullptr;
+    long long total_units = 0, total_vox = 0;
+    unsigned long long* d_counter = nullptr;
+    float4* d_gexp = nullptr;         // all items' accumulators, contiguous
+    size_t gexp_elems = 0;
+    std::vector<size_t> gexp_off;      // [slot][m]
+    int grid[2] = {0, 0};              // persistent grid of the forward, forward + adjoint kernels
+    cudaStream_t capture = nullptr;    // private stream the graphs are recorded on
+    // one graph per kind, valid for the tables, volume pointers and loss
+    // pointer it was recorded with; it runs in the order of the stream it is
+    // launched on
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<ItemDesc> items;
+        std::vector<const float*> vols;
+        float* loss = nullptr;
+    } graph[2];
+};
+
+namespace {
+
+ctfp_status bfail(ctfp_status st, const std::string& m)
+{
+    ctfp::set_last_error(m);
+    return st;
+}
+
+#define BATCH_CUDA(call)                                                                                  \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return bfail(e_ == cudaErrorMemoryAllocation ? CTFP_OOM : CTFP_CUDA_ERROR,                    \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                             \
+    } while (0)
+
+// Records one call's stream work: volume uploads, counter, accumulators,
+// the persistent kernel, the fold.
+ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vols, float* loss, cudaStream_t st)
+{
+    size_t off = 0;
+    for (int s = 0; s < b->n; s++) {
+        ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
+        ctfp_status rs = plan_upload(p, vols.data() + off, st);
+        if (rs != CTFP_OK) return rs;
+        off += (size_t)b->items[(size_t)s].M;
+    }
+    BATCH_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st));
+    if (adjoint) {
+        BATCH_CUDA(cudaMemsetAsync(b->d_gexp, 0, b->gexp_elems * sizeof(float4), st));
+        if (loss) BATCH_CUDA(cudaMemsetAsync(loss, 0, sizeof(float) * (size_t)b->n, st));
+    }
+    BatchArgs a{b->d_items[adjoint ? 1 : 0], b->n, b->total_units, b->d_counter};
+    if (adjoint) k_batch<true><<<b->grid[1], kThreads, 0, st>>>(a);
+    else k_batch<false><<<b->grid[0], kThreads, 0, st>>>(a);
+    BATCH_CUDA(cudaGetLastError());
+    if (adjoint) {
+        long long nb = (b->total_vox + 255) / 256;
+        if (nb > 148 * 16) nb = 148 * 16;
+        k_batch_fold<<<(unsigned)std::max<long long>(nb, 1), 256, 0, st>>>(b->d_items[1], b->n, b->d_vox0,
+                                                                          b->total_vox);
+        BATCH_CUDA(cudaGetLastError());
+    }
+    return CTFP_OK;
+}
+
+// Replays the graph of this kind on st, recording it first (on the batch's
+// private stream: the caller's may be the legacy default stream, which cannot
+// be captured) when the tables, the volume pointers or the loss pointer differ
+// from its recording.
+ctfp_status run(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vols, float* loss, cudaStream_t st)
+{
+    ctfp_batch::Graph& G = b->graph[adjoint ? 1 : 0];
+    const bool same = G.exec && G.loss == loss && G.vols == vols &&
+                      std::memcmp(G.items.data(), b->items.data(), sizeof(ItemDesc) * (size_t)b->n) == 0;
+    if (!same) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+        // the device table changes only here, after the stream's earlier work
+        BATCH_CUDA(cudaStreamSynchronize(st));
+        BATCH_CUDA(cudaMemcpy(b->d_items[adjoint ? 1 : 0], b->items.data(), sizeof(ItemDesc) * (size_t)b->n, cudaMemcpyHostToDevice));
+        cudaGraph_t gr = nullptr;
+        BATCH_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+        const ctfp_status rs = record(b, adjoint, vols, loss, b->capture);
+        const cudaError_t e = cudaStreamEndCapture(b->capture, &gr);
+        if (rs != CTFP_OK) {
+            if (gr) cudaGraphDestroy(gr);
+            return rs;
+        }
+        if (e != cudaSuccess) return bfail(CTFP_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&G.exec, gr, 0);
+        cudaGraphDestroy(gr);
+        if (ei != cudaSuccess) {
+            G.exec = nullptr;
+            return bfail(CTFP_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        G.items = b->items;
+        G.vols = vols;
+        G.loss = loss;
+    }
+    BATCH_CUDA(cudaGraphLaunch(G.exec, st));
+    return CTFP_OK;
+}
+
+struct DevScope {
+    int prev = -1;
+    explicit DevScope(int d)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevScope()
+    {
+        int c = -1;
+        if (prev >= 0 && cudaGetDevice(&c) == cudaSuccess && c != prev) cudaSetDevice(prev);
+    }
+};
+
+// Fills the per-call tables from the plans' current state.
+ctfp_status fill_items(ctfp_batch* b)
+{
+    for (int s = 0; s < b->n; s++) {
+        ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
+        if (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) != SAMPLER_LAYERED)
+            return bfail(CTFP_UNSUPPORTED,
+                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler");
+        if (plan_energies(p) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
+        ItemDesc& it = b->items[(size_t)s];
+        const long long unit0 = it.unit0, units = it.units;
+        std::memset(&it, 0, sizeof(it));
+        it.g = plan_geom(p);
+        it.M = plan_materials(p);
+        it.E = plan_energies(p);
+        it.interp = plan_interp(p);
+        it.mu = plan_mu(p);
+        it.W = plan_W(p);
+        for (int m = 0; m < it.M; m++) {
+            it.ltex[m] = plan_ltex(p, m);
+            it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
+        }
+        it.tiles_u = (it.g.U + kTU - 1) / kTU;
+        it.tiles_v = (it.g.V + kTV - 1) / kTV;
+        it.unit0 = unit0;
+        it.units = units;
+    }
+    return CTFP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_batch** out)
+{
+    if (!out) return bfail(CTFP_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!plans || n_items < 1) return bfail(CTFP_INVALID_ARG, "need at least one plan");
+    for (int i = 0; i < n_items; i++)
+        if (!plans[i]) return bfail(CTFP_INVALID_ARG, "plan is NULL");
+    const int dev = plan_device(plans[0]);
+    for (int i = 0; i < n_items; i++)
+        if (plan_device(plans[i]) != dev) return bfail(CTFP_INVALID_ARG, "plans must share one device");
+    DevScope ds(dev);
+    ctfp_batch* b = new (std::nothrow) ctfp_batch();
+    if (!b) return bfail(CTFP_OOM, "host allocation failed");
+    b->n = n_items;
+    b->device = dev;
+    b->plans.assign(plans, plans + n_items);
+    // cost order: rays x samples x materials, largest first; the queue hands
+    // out units in this order (longest-processing-time-first list scheduling)
+    std::vector<double> cost((size_t)n_items);
+    for (int i = 0; i < n_items; i++) {
+        const GeomParams& g = plan_geom(plans[i]);
+        cost[(size_t)i] = (double)g.U * g.V * g.P * g.K * plan_materials(plans[i]);
+    }
+    b->order.resize((size_t)n_items);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(),
+                     [&](int x, int y) { return cost[(size_t)x] > cost[(size_t)y]; });
+    b->items.resize((size_t)n_items);
+    b->vox0.resize((size_t)n_items);
+    b->gexp_off.assign((size_t)n_items * kMaxM, 0);
+    long long unit = 0, vox = 0;
+    size_t gexp = 0;
+    for (int s = 0; s < n_items; s++) {
+        ctfp_plan* p = plans[b->order[(size_t)s]];
+        const GeomParams& g = plan_geom(p);
+        ItemDesc& it = b->items[(size_t)s];
+        it.unit0 = unit;
+        it.units = (long long)((g.U + kTU - 1) / kTU) * ((g.V + kTV - 1) / kTV) * g.P;
+        unit += it.units;
+        b->vox0[(size_t)s] = vox;
+        vox += (long long)g.nx * g.ny * g.nz;
+        for (int m = 0; m < plan_materials(p); m++) {
+            b->gexp_off[(size_t)s * kMaxM + m] = gexp;
+            gexp += expanded_elems(g);
+        }
+    }
+    b->total_units = unit;
+    b->total_vox = vox;
+    b->gexp_elems = gexp;
+    cudaError_t e = cudaMalloc(&b->d_items[0], sizeof(ItemDesc) * (size_t)n_items);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_items[1], sizeof(ItemDesc) * (size_t)n_items);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_vox0, sizeof(long long) * (size_t)n_items);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_gexp, sizeof(float4) * gexp);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_vox0, b->vox0.data(), sizeof(long long) * (size_t)n_items, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
+    int nsm = 0, per0 = 0, per1 = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per0, k_batch<false>, kThreads, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_batch<true>, kThreads, 0);
+    if (e != cudaSuccess) {
+        ctfp_batch_destroy(b);
+        return bfail(e == cudaErrorMemoryAllocation ? CTFP_OOM : CTFP_CUDA_ERROR,
+                     std::string("ctfp_batch_create: ") + cudaGetErrorString(e));
+    }
+    b->grid[0] = std::max(1, per0) * std::max(1, nsm);
+    b->grid[1] = std::max(1, per1) * std::max(1, nsm);
+    ctfp_status rs = fill_items(b);
+    if (rs != CTFP_OK) {
+        ctfp_batch_destroy(b);
+        return rs;
+    }
+    *out = b;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_batch_destroy(ctfp_batch* b)
+{
+    if (!b) return CTFP_OK;
+    DevScope ds(b->device);
+    for (int i = 0; i < 2; i++)
+        if (b->graph[i].exec) cudaGraphExecDestroy(b->graph[i].exec);
+    cudaFree(b->d_items[0]);
+    cudaFree(b->d_items[1]);
+    cudaFree(b->d_vox0);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_gexp);
+    if (b->capture) cudaStreamDestroy(b->capture);
+    delete b;
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_batch_forward(ctfp_batch* b, const float* const* const* volumes, float* const* I,
+                               float* const* IAbsorb, float* const* L_ckpt, void* stream)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (!volumes || !I) return bfail(CTFP_INVALID_ARG, "volumes and I are required");
+    DevScope ds(b->device);
+    ctfp_status rs = fill_items(b);
+    if (rs != CTFP_OK) return rs;
+    std::vector<const float*> vols;
+    for (int s = 0; s < b->n; s++) {
+        const int k = b->order[(size_t)s];
+        ItemDesc& it = b->items[(size_t)s];
+        if (!volumes[k] || !I[k]) return bfail(CTFP_INVALID_ARG, "NULL volume list or I for an item");
+        for (int m = 0; m < it.M; m++) vols.push_back(volumes[k][m]);
+        it.I = I[k];
+        it.IAbs = IAbsorb ? IAbsorb[k] : nullptr;
+        it.L = L_ckpt ? L_ckpt[k] : nullptr;
+    }
+    return run(b, false, vols, nullptr, (cudaStream_t)stream);
+}
+
+ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* b, const float* const* const* volumes,
+                                       const float* const* I_target, float* const* I, float* const* const* g_volumes,
+                                       float* loss, void* stream)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (!volumes || !I_target || !g_volumes) return bfail(CTFP_INVALID_ARG, "volumes, I_target, g_volumes are required");
+    DevScope ds(b->device);
+    ctfp_status rs = fill_items(b);
+    if (rs != CTFP_OK) return rs;
+    std::vector<const float*> vols;
+    for (int s = 0; s < b->n; s++) {
+        const int k = b->order[(size_t)s];
+        ItemDesc& it = b->items[(size_t)s];
+        if (!volumes[k] || !I_target[k] || !g_volumes[k])
+            return bfail(CTFP_INVALID_ARG, "NULL volume list, target or gradient list for an item");
+        for (int m = 0; m < it.M; m++) {
+            if (!g_volumes[k][m]) return bfail(CTFP_INVALID_ARG, "NULL gradient volume");
+            vols.push_back(volumes[k][m]);
+            it.gvol[m] = g_volumes[k][m];
+        }
+        it.I = I ? I[k] : nullptr;
+        it.I_target = I_target[k];
+        it.loss = loss ? loss + k : nullptr;
+    }
+    return run(b, true, vols, loss, (cudaStream_t)stream);
+}
+
+ctfp_status ctfp_batch_info(const ctfp_batch* b, int64_t* total_units, int32_t* grid_forward, int32_t* grid_adjoint)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (total_units) *total_units = b->total_units;
+    if (grid_forward) *grid_forward = b->grid[0];
+    if (grid_adjoint) *grid_adjoint = b->grid[1];
+    return CTFP_OK;
+}
+
+}  // extern "C"

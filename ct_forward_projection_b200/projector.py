@@ -119,6 +119,19 @@ class Projector:
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)
 
+    def autotune(self, volumes: Sequence, n_sample_views: int = 16, stream=None) -> dict:
+        """ctfp_plan_autotune: times launch shapes on a sample of views and
+        sets the fastest; returns it with its time and whether it was cached."""
+        import torch
+        P, V, U = self.shape_proj
+        dev = f"cuda:{self.device}"
+        I = torch.empty((P, V, U), device=dev)
+        A = torch.empty((P, V, U), device=dev)
+        r = capi.LaunchShape()
+        call("ctfp_plan_autotune", self._h, self._vol_ptrs(volumes), _dptr(I), _dptr(A), int(n_sample_views),
+             C.byref(r), _stream(stream))
+        return {k: getattr(r, k) for k, _ in capi.LaunchShape._fields_}
+
     # -- tables -------------------------------------------------------------
     def set_spectral_tables(self, spectrum, mu, grid=None, grid_layout: int | None = None, det_response=None,
                             I0Val: float = 60000.0) -> None:
@@ -221,6 +234,81 @@ class Projector:
         n = C.c_int64()
         call("ctfp_count_support_samples", self._h, C.byref(n))
         return int(n.value)
+
+
+class Batch:
+    """ctfp_batch: several plans in one persistent launch replayed as a CUDA
+    graph.  Keeps references to its projectors; close it before them."""
+
+    def __init__(self, projectors: Sequence[Projector]):
+        self.projectors = list(projectors)
+        plans = ptr_array([p.handle.value for p in self.projectors])
+        h = C.c_void_p()
+        call("ctfp_batch_create", len(self.projectors), plans, C.byref(h))
+        self._h = h
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ctfp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        u, g0, g1 = C.c_int64(), C.c_int32(), C.c_int32()
+        call("ctfp_batch_info", self._h, C.byref(u), C.byref(g0), C.byref(g1))
+        return {"units": int(u.value), "grid_forward": int(g0.value), "grid_adjoint": int(g1.value)}
+
+    def _vol_table(self, volumes):
+        assert len(volumes) == len(self.projectors)
+        per = [p._vol_ptrs(v) for p, v in zip(self.projectors, volumes)]
+        self._keep = per
+        return ptr_array([C.cast(a, C.c_void_p).value for a in per])
+
+    def _out(self, want_L: bool = False) -> list:
+        import torch
+        outs = []
+        for p in self.projectors:
+            dev = f"cuda:{p.device}"
+            P, V, U = p.shape_proj
+            o = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
+            if want_L:
+                o["L"] = torch.empty((P, V, U, p.M), device=dev)
+            outs.append(o)
+        return outs
+
+    def forward(self, volumes: Sequence[Sequence], want_L: bool = False, out: list | None = None, stream=None) -> list:
+        """volumes[k] = the M density maps of item k; returns [dict(I, IAbsorb[, L])]."""
+        out = out if out is not None else self._out(want_L)
+        vt = self._vol_table(volumes)
+        I = ptr_array([_dptr(o["I"]) for o in out])
+        A = ptr_array([_dptr(o.get("IAbsorb")) for o in out])
+        L = ptr_array([_dptr(o.get("L")) for o in out]) if any("L" in o for o in out) else None
+        call("ctfp_batch_forward", self._h, vt, I, A, L, _stream(stream))
+        return out
+
+    def forward_adjoint(self, volumes: Sequence[Sequence], targets: Sequence, grads: list | None = None,
+                        I_out: list | None = None, loss=None, stream=None) -> dict:
+        """Fused forward + sum (log I - log T)^2 + adjoint; grads accumulate."""
+        import torch
+        if grads is None:
+            grads = [[torch.zeros(p.shape_vol, device=f"cuda:{p.device}") for _ in range(p.M)]
+                     for p in self.projectors]
+        if loss is None:
+            loss = torch.zeros(len(self.projectors), device=f"cuda:{self.projectors[0].device}")
+        vt = self._vol_table(volumes)
+        gtabs = [ptr_array([_dptr(g) for g in gk]) for gk in grads]
+        self._keep = self._keep + gtabs
+        G = ptr_array([C.cast(a, C.c_void_p).value for a in gtabs])
+        T = ptr_array([_dptr(t) for t in targets])
+        I = ptr_array([_dptr(t) for t in I_out]) if I_out is not None else None
+        call("ctfp_batch_forward_adjoint", self._h, vt, T, I, G, _dptr(loss), _stream(stream))
+        return {"grads": grads, "loss": loss, "I": I_out}
 
 
 def _host_ptr(a):

@@ -198,6 +198,64 @@ ctfp_status ctfp_backward(ctfp_plan* plan, const float* L_ckpt, const float* gI,
 ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float* const* g_volumes,
                                         void* stream);
 
+/* ---- launch-shape autotuner ------------------------------------------------
+ * No counterpart in the reference (fixed 8 x 8 x 8 blocks,
+ * Source/CUDAFun/CBCTPolyProjGPU.cuh:22-24).  Times candidate launch shapes of
+ * the fused forward (tiles 8 x 8 ... 64 x 4, 2-4 CTAs per SM, 1-4 views per CTA)
+ * on n_sample_views views (0: 16) in four chunks spread round the rotation, and
+ * sets the fastest on the plan (as ctfp_plan_set_launch_shape).  I and IAbsorb
+ * are full-size output buffers as for ctfp_forward; their contents are
+ * undefined afterwards.  Synchronises the stream.  Results are cached per
+ * process by geometry, materials, sampler, energies and device name, and in the
+ * text file named by the environment variable CTFP_TUNE_CACHE when it is set. */
+typedef struct ctfp_launch_shape {
+    int32_t tile_u, tile_v, views_per_cta, min_ctas_per_sm;
+    float ms;            /* time of the sampled views with this shape */
+    int32_t from_cache;  /* 1 when no timing ran */
+} ctfp_launch_shape;
+ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, float* I, float* IAbsorb,
+                               int32_t n_sample_views, ctfp_launch_shape* out, void* stream);
+
+/* ---- batched form -------------------------------------------------------------
+ * No counterpart in the reference, which simulates one phantom per process run
+ * (main.cpp:4-8).  A batch holds n_items plans (own geometry, materials,
+ * spectral tables; one device) and runs all of them in ONE persistent launch
+ * over a device work queue: a work unit is one view x one 16 x 8 detector
+ * tile; items are queued largest first (rays x samples x materials), each CTA
+ * takes the next unit from an atomic counter.  A call is recorded once as a
+ * CUDA graph (volume uploads, queue reset, kernel, fold) and replayed, in the
+ * order of the stream passed, while the item pointers and the plans' tables
+ * stay the same; a change re-records it (one host synchronisation).  The batch
+ * uploads into the plans' own texture arrays: do not run a batch and its plans
+ * concurrently.
+ *
+ * Items must use CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered
+ * sampler (the default) and have spectral tables set.  The batch keeps the
+ * plans' pointers: destroy it before them.  Arrays indexed by item follow the
+ * order of `plans`. */
+typedef struct ctfp_batch ctfp_batch;
+ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_batch** out);
+ctfp_status ctfp_batch_destroy(ctfp_batch* batch);
+
+/* Per item k: the same outputs as ctfp_forward(plans[k], volumes[k], I[k],
+ * IAbsorb[k], NULL, L_ckpt[k]).  IAbsorb and L_ckpt may be NULL (whole array)
+ * or hold NULL entries. */
+ctfp_status ctfp_batch_forward(ctfp_batch* batch, const float* const* const* volumes, float* const* I,
+                               float* const* IAbsorb, float* const* L_ckpt, void* stream);
+
+/* Fused forward + loss + adjoint.  Per item k and ray r, with I_r the forward
+ * intensity and T_r = I_target[k][r] > 0:
+ *   loss[k]         = sum_r (log I_r - log T_r)^2            (device, may be NULL)
+ *   g_volumes[k][m] += d loss[k] / d volumes[k][m]           (accumulated)
+ * rays with I_r <= 0 contribute nothing.  I (may be NULL) receives I_r. */
+ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* const* volumes,
+                                       const float* const* I_target, float* const* I,
+                                       float* const* const* g_volumes, float* loss, void* stream);
+
+/* Work units in the queue, persistent grid sizes of the two kernels. */
+ctfp_status ctfp_batch_info(const ctfp_batch* batch, int64_t* total_units, int32_t* grid_forward,
+                            int32_t* grid_adjoint);
+
 /* ---- forward without device allocation -------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code running inside a host framework that owns all device memory through its

@@ -113,3 +113,42 @@ def test_backward_central_differences(cuda_ok):
         scale = max(abs(fd), 1e-3 * np.max(np.abs(g[m])))
         worst = max(worst, abs(g[m][idx] - fd) / scale)
     assert worst < 2e-2
+
+
+def test_autograd_binding(cuda_ok):
+    # project() through torch.autograd equals ctfp_backward with the same
+    # dLoss/dI, dLoss/dIAbsorb, and its directional derivative matches FP64
+    # central differences of the oracle loss
+    from ct_forward_projection_b200.autograd import project
+    d = small_geometry(n=(11, 10, 9), views=3, U=12, V=9)
+    M = 2
+    vols = random_volumes(d, M, 71)
+    S, mu, G, D = spectral_setup(d, M, 6, 8)
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    target = O.forward(d, [v * np.float32(0.95) for v in vols], mu, W)["I"]
+    logt = torch.from_numpy(np.log(target)).cuda().float()
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        xs = [torch.from_numpy(v).cuda().requires_grad_(True) for v in vols]
+        I, A, I0 = project(pr, *xs)
+        loss = torch.sum((torch.log(I) - logt.view(I.shape)) ** 2) + 1e-4 * torch.sum(A)
+        loss.backward()
+        f = pr.forward(to_dev(vols), want_L=True)
+        gI = 2.0 * (torch.log(f["I"]) - logt.view(I.shape)) / f["I"]
+        ref = pr.backward(f["L"], gI=gI, gIAbsorb=torch.full_like(f["I"], 1e-4))
+        torch.cuda.synchronize()
+        assert not I0.requires_grad
+    for m in range(M):
+        assert torch.max(torch.abs(xs[m].grad - ref[m])) / torch.max(torch.abs(ref[m])) < 1e-5
+    rng = np.random.RandomState(3)
+    dirs = [rng.normal(size=v.shape) for v in vols]
+
+    def f64_loss(t):
+        vs = [(v.astype(np.float64) + t * dv).astype(np.float32) for v, dv in zip(vols, dirs)]
+        r = O.forward(d, vs, mu, W)
+        return float(np.sum((np.log(r["I"]) - np.log(target)) ** 2) + 1e-4 * np.sum(r["IAbsorb"]))
+
+    h = 1e-3
+    fd = (f64_loss(h) - f64_loss(-h)) / (2 * h)
+    an = sum(float(np.sum(xs[m].grad.double().cpu().numpy() * dirs[m])) for m in range(M))
+    assert abs(an - fd) / abs(fd) < 1e-2
