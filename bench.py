@@ -207,6 +207,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--batch-items", type=int, default=48,
+                    help="problems in the uneven batch leg (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -246,6 +249,11 @@ def main():
     rays = P * U * V
     out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
     stream = torch.cuda.current_stream()
+    shape = {"tile_u": 16, "tile_v": 8, "views_per_cta": 2, "min_ctas_per_sm": 4, "source": "default"}
+    if not args.no_autotune:
+        r = pr.autotune(vols, n_sample_views=16)
+        shape = {k: r[k] for k in ("tile_u", "tile_v", "views_per_cta", "min_ctas_per_sm")}
+        shape["source"] = "cache" if r["from_cache"] else "autotuned"
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
     # ---------------- device-resident forward (value) -----------------------
@@ -321,6 +329,11 @@ def main():
         fa_ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
         fa = {"value": ws * rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms}
 
+    # ---------------- uneven batch: batched vs loop of plain calls ----------
+    batch = None
+    if args.batch_items > 0:
+        batch = batch_leg(args, ws, rank, local, stream)
+
     # ---------------- CPU baseline (rank 0, N = 1) --------------------------
     cpu = None
     err = None
@@ -344,6 +357,8 @@ def main():
             "cpu_baseline": cpu,
             "max_rel_err_vs_fp64_oracle": err,
             "fwd_adjoint": fa,
+            "batch": batch,
+            "launch_shape": shape,
             "gpu_launches": args.steps,
             "clocks": clk,
         }
@@ -353,6 +368,114 @@ def main():
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def batch_leg(args, ws, rank, local, stream):
+    """The uneven batch (physics.batch_workloads): every problem forward, and
+    forward + loss sum (log I - log T)^2 + adjoint, as one graph-replayed
+    persistent launch (ctfp_batch_*) against a loop of plain calls (ctfp_forward,
+    dLoss/dI in torch, ctfp_backward) over the same problems.  One untimed
+    warm-up (records the graphs) and one timed pass per arm; L2 is irrelevant
+    at these sizes (tens of GB per pass)."""
+    import torch
+
+    from ct_forward_projection_b200 import physics
+    from ct_forward_projection_b200.projector import Batch, Projector
+    dev = f"cuda:{local}"
+    wl = physics.batch_workloads(args.batch_items, seed=4000 + 97 * rank)
+    prs, vols, outs, Ls, targets, grads_loop, grads_b = [], [], [], [], [], [], []
+    rays = 0
+    for w in wl:
+        pr = Projector(w.geometry, len(w.materials), "trilinear", local)
+        pr.set_tables_from_workload(w)
+        v = physics.phantom(w, dev)
+        P, V, U = pr.shape_proj
+        prs.append(pr)
+        vols.append(v)
+        outs.append({"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)})
+        Ls.append(torch.empty((P, V, U, pr.M), device=dev))
+        grads_loop.append([torch.zeros_like(x) for x in v])
+        grads_b.append([torch.zeros_like(x) for x in v])
+        rays += P * V * U
+    # targets: the plain forward of each problem, perturbed multiplicatively
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(11 + rank)
+    for pr, v, o in zip(prs, vols, outs):
+        pr.forward(v, out=o)
+        targets.append(o["I"] * torch.exp(0.05 * torch.randn(o["I"].shape, device=dev, generator=gen)))
+    b = Batch(prs)
+    b_outs = [{"I": torch.empty_like(o["I"]), "IAbsorb": torch.empty_like(o["I"])} for o in outs]
+    b_I = [torch.empty_like(o["I"]) for o in outs]
+    loss_b = torch.zeros(len(prs), device=dev)
+
+    def loop_fwd():
+        for pr, v, o in zip(prs, vols, outs):
+            pr.forward(v, out=o)
+
+    def loop_fwd_adj():
+        for pr, v, o, L, T, g in zip(prs, vols, outs, Ls, targets, grads_loop):
+            pr.forward(v, out={**o, "L": L})
+            gI = 2.0 * (torch.log(o["I"]) - torch.log(T)) / o["I"]
+            pr.backward(L, gI=gI, grads=g)
+
+    def batched_fwd():
+        b.forward(vols, out=b_outs)
+
+    def batched_fwd_adj():
+        b.forward_adjoint(vols, targets, grads=grads_b, I_out=b_I, loss=loss_b)
+
+    def timed(fn):
+        fn()  # warm-up (records the batch's graph)
+        barrier_sync(ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        barrier_sync(ws)
+        return max_over_ranks(e0.elapsed_time(e1), ws)
+
+    t_loop_f = timed(loop_fwd)
+    t_b_f = timed(batched_fwd)
+    for g in grads_loop + grads_b:
+        for x in g:
+            x.zero_()
+    t_loop_fa = timed(loop_fwd_adj)
+    t_b_fa = timed(batched_fwd_adj)
+    torch.cuda.synchronize()
+    # both arms ran twice: gradients hold two passes each
+    gerr = max(float(torch.max(torch.abs(a - c)) / torch.max(torch.abs(c)).clamp_min(1e-30))
+               for ga, gc in zip(grads_b, grads_loop) for a, c in zip(ga, gc))
+    ierr = max(float(torch.max(torch.abs(a["I"] - c["I"]) / c["I"].abs().clamp_min(1e-30)))
+               for a, c in zip(b_outs, outs))
+    # the batched forward against the FP64 oracle on seeded rays of three problems
+    oerr = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import oracle as O
+        oerr = 0.0
+        rng = np.random.RandomState(3)
+        for k in (0, len(wl) // 2, len(wl) - 1):
+            w = wl[k]
+            W = _weights_from_tables(w, local)
+            ids = np.sort(rng.choice(w.n_rays, 1024, replace=False))
+            ref = O.forward(w.geometry, [x.cpu().numpy() for x in vols[k]], w.mu_table(), W, O.TRILINEAR, ids)
+            got = b_outs[k]["I"].reshape(-1)[torch.from_numpy(ids).to(dev)].double().cpu().numpy()
+            oerr = max(oerr, float(np.max(np.abs(got - ref["I"]) / np.abs(ref["I"]))))
+    info = b.info()
+    b.close()
+    for pr in prs:
+        pr.close()
+    n_rays = ws * rays
+    return {
+        "items": len(wl), "rays_per_pass": rays, "work_units": info["units"],
+        "persistent_grid": [info["grid_forward"], info["grid_adjoint"]],
+        "fwd": {"loop_rays_s": n_rays / (t_loop_f / 1e3), "batched_rays_s": n_rays / (t_b_f / 1e3),
+                "loop_ms": t_loop_f, "batched_ms": t_b_f, "speedup": t_loop_f / t_b_f},
+        "fwd_adjoint": {"loop_rays_s": n_rays / (t_loop_fa / 1e3), "batched_rays_s": n_rays / (t_b_fa / 1e3),
+                        "loop_ms": t_loop_fa, "batched_ms": t_b_fa, "speedup": t_loop_fa / t_b_fa},
+        "max_rel_diff_I_batched_vs_loop": ierr, "max_rel_diff_grad_batched_vs_loop": gerr,
+        "max_rel_err_batched_I_vs_fp64_oracle": oerr,
+        "note": "one warm-up + one timed pass per arm; loop = ctfp_forward + torch dLoss/dI + ctfp_backward per problem",
+    }
 
 
 def _weights_from_tables(w, device):

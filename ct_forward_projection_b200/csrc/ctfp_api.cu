@@ -411,7 +411,7 @@ ctfp_status ctfp_plan_set_interp(ctfp_plan* p, int32_t interp)
 ctfp_status ctfp_plan_set_sampler(ctfp_plan* p, int32_t sampler)
 {
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
-    if (sampler != CTFP_SAMPLER_GLOBAL && sampler != CTFP_SAMPLER_LAYERED)
+    if (sampler != CTFP_SAMPLER_GLOBAL && sampler != CTFP_SAMPLER_LAYERED && sampler != CTFP_SAMPLER_BRICK)
         return fail(CTFP_INVALID_ARG, "unknown sampler");
     if (sampler == CTFP_SAMPLER_LAYERED && p->geom.pNumZ > 2048)
         return fail(CTFP_UNSUPPORTED, "layered sampler holds at most 2048 z slices");

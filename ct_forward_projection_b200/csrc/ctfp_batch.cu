@@ -1,21 +1,25 @@
 // ctfp_batch.cu — the batched form: many independent problems (their own
-// geometry, materials, spectra, view counts) in one persistent launch over a
-// work queue, replayed as a CUDA graph.  No reference counterpart.
+// geometry, materials, spectra, view counts) run by persistent kernels over a
+// device work queue, the whole call replayed as one CUDA graph.  No reference
+// counterpart.
 //
-// Work unit = (item, view, 16 x 8 pixel tile).  The persistent grid is sized
-// to the device's residency; each CTA takes units from a global counter
-// (atomicAdd, no waits), items ordered by estimated cost, largest first, so
-// the long problems start early and the short ones fill the tail.
+// Work unit = (item, view, 8 x 4 pixel patch): the 32 rays of one warp.  Items
+// are grouped by material count and sampler mode (one kernel instantiation
+// each, so every group runs with the registers its own march needs); within a
+// group they are queued largest first (rays x samples x materials), and every
+// warp takes the next unit from the group's counter (atomicAdd, no waits, no
+// block barriers), so long problems start early, short ones fill the tail,
+// and a warp whose rays were short moves on at once.
 //
-// Two kernels run per batch: the forward (march + spectral epilogue, optional
-// checkpoint), and the fused forward + loss + adjoint, which for every ray
-// marches, forms I, the loss sum (log I - log I_target)^2 and its gradient,
-// the spectral-weight recompute, and the adjoint march scattering into the
-// corner-expanded accumulators (two 16-byte vector reductions per sample and
-// material); a fold kernel then adds the accumulators into the gradients.
+// Two kinds of call: the forward (march + spectral epilogue, optional
+// checkpoint) and the fused forward + loss + adjoint, which for every ray
+// marches, forms I, the loss term (log I - log I_target)^2 and its gradient,
+// recomputes the spectral weights, and marches again scattering into the
+// corner-expanded accumulators; a fold kernel then adds the accumulators into
+// the gradients.
 #include <algorithm>
-#include <new>
 #include <cstring>
+#include <new>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -41,18 +45,19 @@ using namespace ctfp;
 
 namespace {
 
-constexpr int kTU = 16, kTV = 8, kThreads = kTU * kTV;
+constexpr int kPU = 8, kPV = 4;       // rays of one unit (one warp): u x v
+constexpr int kWarps = 4, kThreads = 32 * kWarps;
 
 // One item as the persistent kernels see it.  The pointer fields are refreshed
-// per call from the batch's staging table.
+// per call.
 struct ItemDesc {
     GeomParams g;
     cudaTextureObject_t ltex[kMaxM];
     const float* mu;   // [E][M]
     const float* W;    // [E][V][U]
     int M, E, interp;
-    int tiles_u, tiles_v;
-    long long unit0;   // first global unit of this item
+    int patches_u, patches_v;
+    long long unit0;   // first unit of this item in the batch's numbering
     long long units;
     // per call
     float* I;
@@ -64,16 +69,17 @@ struct ItemDesc {
     float* loss;       // device scalar accumulated with atomicAdd
 };
 
-struct BatchArgs {
+// One group: items [first, first + count) of the table, units [begin, end).
+struct GroupArgs {
     const ItemDesc* items;
-    int n_items;
-    long long total_units;
+    int first, count;
+    long long begin, end;
     unsigned long long* counter;
 };
 
-__device__ __forceinline__ int find_item(const BatchArgs& a, long long unit)
+__device__ __forceinline__ int find_item(const GroupArgs& a, long long unit)
 {
-    int lo = 0, hi = a.n_items - 1;
+    int lo = a.first, hi = a.first + a.count - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (a.items[mid].unit0 <= unit) lo = mid;
@@ -82,61 +88,57 @@ __device__ __forceinline__ int find_item(const BatchArgs& a, long long unit)
     return lo;
 }
 
-__device__ __forceinline__ long long next_unit(const BatchArgs& a, long long* s_unit)
+template <int MODE>
+__device__ __forceinline__ Corner batch_corner(const ItemDesc& it, const RaySeg& s, const RayRef32& r, int i)
 {
-    __syncthreads();
-    if (threadIdx.x == 0) *s_unit = (long long)atomicAdd(a.counter, 1ull);
-    __syncthreads();
-    return *s_unit;
+    if (MODE == INTERP_TRILINEAR) {
+        const double t = (double)i;
+        return corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+    }
+    return corner_tex(ref32_coords(it.g, r, i));
 }
 
 // Path integrals of one ray through the layered sampler.
 template <int M, int MODE>
-__device__ __forceinline__ void batch_march(const ItemDesc& it, int p, int v, int u, float* L)
+__device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s, const RayRef32& r, float* L)
 {
-    const RaySeg s = ray_segment(it.g, p, v, u);
     float acc[M], cmp[M];
 #pragma unroll
     for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
-    const RayRef32 r = ray_ref32(it.g, p, v, u);
+#pragma unroll 2
     for (int i = s.i0; i < s.i1; i++) {
-        const double t = (double)i;
-        const Corner c = MODE == INTERP_TRILINEAR
-                             ? corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az))
-                             : corner_tex(ref32_coords(it.g, r, i));
-        float val[M];
-        gather4_interp<M, MODE>(it.ltex, it.g.nz, c, val);
+        const Corner c = batch_corner<MODE>(it, s, r, i);
+        float v[M][8];
+        load8_layered<M>(it.ltex, it.g.nz, c, v);
 #pragma unroll
-        for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+        for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], interp8<MODE>(c, v[m]));
     }
 #pragma unroll
     for (int m = 0; m < M; m++) L[m] = it.g.dx * (acc[m] - cmp[m]);
 }
 
 template <int M, int MODE>
-__device__ __forceinline__ void batch_scatter(const ItemDesc& it, int p, int v, int u, const float* g)
+__device__ __forceinline__ void batch_scatter(const ItemDesc& it, const RaySeg& s, const RayRef32& r, const float* g)
 {
-    const RaySeg s = ray_segment(it.g, p, v, u);
-    const RayRef32 r = ray_ref32(it.g, p, v, u);
-    for (int i = s.i0; i < s.i1; i++) {
-        const double t = (double)i;
-        const Corner c = MODE == INTERP_TRILINEAR
-                             ? corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az))
-                             : corner_tex(ref32_coords(it.g, r, i));
-        scatter_expanded<M, MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(it.gexp, it.g.nx, it.g.ny,
-                                                                                         it.g.nz, c, g);
-    }
+    ScatterRun<M> run;
+    for (int i = s.i0; i < s.i1; i++)
+        run.template add<MODE>(it.gexp, it.g.nx, it.g.ny, it.g.nz, batch_corner<MODE>(it, s, r, i), g);
+    run.flush(it.gexp, it.g.nx, it.g.ny, it.g.nz);
 }
 
-// One ray of one unit.  ADJOINT: the fused forward + loss + adjoint.
+// One ray.  ADJOINT: the fused forward + loss + adjoint; returns the ray's
+// loss term.
 template <int M, int MODE, bool ADJOINT>
 __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_mu, int p, int v, int u)
 {
     const int64_t npix = (int64_t)it.g.U * it.g.V;
     const int64_t pix = (int64_t)v * it.g.U + u;
     const int64_t ray = (int64_t)p * npix + pix;
+    const RaySeg s = ray_segment(it.g, p, v, u);
+    RayRef32 r;
+    if (MODE != INTERP_TRILINEAR) r = ray_ref32(it.g, p, v, u);
     float L[M];
-    batch_march<M, MODE>(it, p, v, u, L);
+    batch_march<M, MODE>(it, s, r, L);
     float sI = 0.f, cI = 0.f, sA = 0.f, cA = 0.f, S[M];
 #pragma unroll
     for (int m = 0; m < M; m++) S[m] = 0.f;
@@ -155,7 +157,7 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
         }
         const float Ie = w * ex;
         kahan_add(sI, cI, Ie);
-        kahan_add(sA, cA, w * om);
+        if (!ADJOINT) kahan_add(sA, cA, w * om);
         if (ADJOINT) {
 #pragma unroll
             for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
@@ -163,13 +165,15 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     }
     const float I = sI - cI;
     if (it.I) it.I[ray] = I;
-    if (it.IAbs) it.IAbs[ray] = sA - cA;
-    if (it.L) {
+    if (!ADJOINT) {
+        if (it.IAbs) it.IAbs[ray] = sA - cA;
+        if (it.L) {
 #pragma unroll
-        for (int m = 0; m < M; m++) it.L[ray * M + m] = L[m];
+            for (int m = 0; m < M; m++) it.L[ray * M + m] = L[m];
+        }
+        return 0.f;
     }
-    if (!ADJOINT) return 0.f;
-    // loss (log I - log I_t)^2 and dLoss/dI = 2 (log I - log I_t) / I; dI/dL_m = -S_m
+    // loss (log I - log T)^2: dLoss/dI = 2 (log I - log T) / I, dI/dL_m = -S_m
     if (!(I > 0.f)) return 0.f;
     const float res = logf(I) - logf(it.I_target[ray]);
     const float gI = 2.0f * res / I;
@@ -180,58 +184,49 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
         g[m] = -gI * S[m] * it.g.dx;
         any |= g[m] != 0.f;
     }
-    if (any) batch_scatter<M, MODE>(it, p, v, u, g);
+    if (any) batch_scatter<M, MODE>(it, s, r, g);
     return res * res;
 }
 
-// Residency: forward 6 CTAs of 128 threads per SM (80 registers, no spill);
-// the fused adjoint 5 (the scatter needs more registers).
-template <bool ADJOINT>
-__global__ void __launch_bounds__(kThreads, ADJOINT ? 5 : 6) k_batch(const BatchArgs a)
+// CTAs of 128 threads per SM the kernels are compiled for (their register
+// caps: 65536 / (128 * minb)); the fused adjoint carries the scatter's run
+// accumulators on top of the march.
+template <bool ADJOINT, int M>
+struct BatchBudget {
+    static constexpr int minb = ADJOINT ? (M <= 2 ? 5 : 4) : (M <= 2 ? 8 : 6);
+};
+
+template <int M, int MODE, bool ADJOINT>
+__global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M>::minb) k_batch(const GroupArgs a)
 {
-    __shared__ float s_mu[CTFP_MAX_ENERGIES * kMaxM];
-    __shared__ long long s_unit;
-    __shared__ float s_loss[kThreads / 32];
+    __shared__ float s_mu_all[kWarps][CTFP_MAX_ENERGIES * M];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* s_mu = s_mu_all[warp];
     int cached = -1;
     for (;;) {
-        const long long unit = next_unit(a, &s_unit);
-        if (unit >= a.total_units) break;
+        long long unit = 0;
+        if (lane == 0) unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= a.end) break;
         const int k = find_item(a, unit);
         const ItemDesc& it = a.items[k];
         if (k != cached) {
-            for (int j = threadIdx.x; j < it.E * it.M; j += blockDim.x) s_mu[j] = it.mu[j];
+            __syncwarp();
+            for (int j = lane; j < it.E * M; j += 32) s_mu[j] = it.mu[j];
+            __syncwarp();
             cached = k;
-            __syncthreads();
         }
         const long long local = unit - it.unit0;
-        const int tiles = it.tiles_u * it.tiles_v;
-        const int p = (int)(local / tiles);
-        const int tile = (int)(local % tiles);
-        const int u = (tile % it.tiles_u) * kTU + (int)(threadIdx.x % kTU);
-        const int v = (tile / it.tiles_u) * kTV + (int)(threadIdx.x / kTU);
+        const int patches = it.patches_u * it.patches_v;
+        const int p = (int)(local / patches);
+        const int patch = (int)(local % patches);
+        const int u = (patch % it.patches_u) * kPU + (lane % kPU);
+        const int v = (patch / it.patches_u) * kPV + (lane / kPU);
         float loss = 0.f;
-        if (u < it.g.U && v < it.g.V) {
-            const bool tri = it.interp == INTERP_TRILINEAR;
-            switch (it.M) {
-                case 1: loss = tri ? process_ray<1, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
-                                   : process_ray<1, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
-                case 2: loss = tri ? process_ray<2, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
-                                   : process_ray<2, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
-                case 3: loss = tri ? process_ray<3, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
-                                   : process_ray<3, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
-                default: loss = tri ? process_ray<4, INTERP_TRILINEAR, ADJOINT>(it, s_mu, p, v, u)
-                                    : process_ray<4, INTERP_TEXEMU, ADJOINT>(it, s_mu, p, v, u); break;
-            }
-        }
+        if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT>(it, s_mu, p, v, u);
         if (ADJOINT && it.loss) {
             for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
-            if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = loss;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                float t = 0.f;
-                for (int w = 0; w < kThreads / 32; w++) t += s_loss[w];
-                atomicAdd(it.loss, t);
-            }
+            if (lane == 0) atomicAdd(it.loss, loss);
         }
     }
 }
@@ -260,23 +255,42 @@ __global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long
     }
 }
 
+using KernelFn = void (*)(GroupArgs);
+
+template <bool ADJOINT>
+KernelFn kernel_for(int M, int interp)
+{
+    const bool tri = interp == INTERP_TRILINEAR;
+    switch (M) {
+        case 1: return tri ? k_batch<1, INTERP_TRILINEAR, ADJOINT> : k_batch<1, INTERP_TEXEMU, ADJOINT>;
+        case 2: return tri ? k_batch<2, INTERP_TRILINEAR, ADJOINT> : k_batch<2, INTERP_TEXEMU, ADJOINT>;
+        case 3: return tri ? k_batch<3, INTERP_TRILINEAR, ADJOINT> : k_batch<3, INTERP_TEXEMU, ADJOINT>;
+        default: return tri ? k_batch<4, INTERP_TRILINEAR, ADJOINT> : k_batch<4, INTERP_TEXEMU, ADJOINT>;
+    }
+}
+
 }  // namespace
 
 struct ctfp_batch {
     int n = 0;
     int device = 0;
     std::vector<ctfp_plan*> plans;
-    std::vector<int> order;            // item slots in cost order
+    std::vector<int> order;            // item slot -> plan index (grouped, cost order within a group)
     std::vector<long long> vox0;       // first voxel of each slot in the fold's flat index
     std::vector<ItemDesc> items;       // tables of the current call
+    struct Group {
+        int M, interp, first, count;
+        long long begin, end;
+        int grid[2];                   // persistent grid: forward, forward + adjoint
+    };
+    std::vector<Group> groups;
     ItemDesc* d_items[2] = {nullptr, nullptr};  // device tables of the forward, forward + adjoint graphs
     long long* d_vox0 = nullptr;
     long long total_units = 0, total_vox = 0;
-    unsigned long long* d_counter = nullptr;
-    float4* d_gexp = nullptr;         // all items' accumulators, contiguous
+    unsigned long long* d_counter = nullptr;    // one per group
+    float4* d_gexp = nullptr;          // all items' accumulators, contiguous
     size_t gexp_elems = 0;
     std::vector<size_t> gexp_off;      // [slot][m]
-    int grid[2] = {0, 0};              // persistent grid of the forward, forward + adjoint kernels
     cudaStream_t capture = nullptr;    // private stream the graphs are recorded on
     // one graph per kind, valid for the tables, volume pointers and loss
     // pointer it was recorded with; it runs in the order of the stream it is
@@ -305,8 +319,8 @@ ctfp_status bfail(ctfp_status st, const std::string& m)
                          std::string(#call) + ": " + cudaGetErrorString(e_));                             \
     } while (0)
 
-// Records one call's stream work: volume uploads, counter, accumulators,
-// the persistent kernel, the fold.
+// Records one call's stream work: volume uploads, counters, accumulators, the
+// persistent kernel of every group, the fold.
 ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vols, float* loss, cudaStream_t st)
 {
     size_t off = 0;
@@ -316,20 +330,23 @@ ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>&
         if (rs != CTFP_OK) return rs;
         off += (size_t)b->items[(size_t)s].M;
     }
-    BATCH_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), st));
+    BATCH_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * b->groups.size(), st));
     if (adjoint) {
         BATCH_CUDA(cudaMemsetAsync(b->d_gexp, 0, b->gexp_elems * sizeof(float4), st));
         if (loss) BATCH_CUDA(cudaMemsetAsync(loss, 0, sizeof(float) * (size_t)b->n, st));
     }
-    BatchArgs a{b->d_items[adjoint ? 1 : 0], b->n, b->total_units, b->d_counter};
-    if (adjoint) k_batch<true><<<b->grid[1], kThreads, 0, st>>>(a);
-    else k_batch<false><<<b->grid[0], kThreads, 0, st>>>(a);
-    BATCH_CUDA(cudaGetLastError());
+    const ItemDesc* table = b->d_items[adjoint ? 1 : 0];
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+        const ctfp_batch::Group& G = b->groups[gi];
+        GroupArgs a{table, G.first, G.count, G.begin, G.end, b->d_counter + gi};
+        KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp) : kernel_for<false>(G.M, G.interp);
+        fn<<<G.grid[adjoint ? 1 : 0], kThreads, 0, st>>>(a);
+        BATCH_CUDA(cudaGetLastError());
+    }
     if (adjoint) {
         long long nb = (b->total_vox + 255) / 256;
         if (nb > 148 * 16) nb = 148 * 16;
-        k_batch_fold<<<(unsigned)std::max<long long>(nb, 1), 256, 0, st>>>(b->d_items[1], b->n, b->d_vox0,
-                                                                          b->total_vox);
+        k_batch_fold<<<(unsigned)std::max<long long>(nb, 1), 256, 0, st>>>(table, b->n, b->d_vox0, b->total_vox);
         BATCH_CUDA(cudaGetLastError());
     }
     return CTFP_OK;
@@ -349,7 +366,8 @@ ctfp_status run(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vo
         G.exec = nullptr;
         // the device table changes only here, after the stream's earlier work
         BATCH_CUDA(cudaStreamSynchronize(st));
-        BATCH_CUDA(cudaMemcpy(b->d_items[adjoint ? 1 : 0], b->items.data(), sizeof(ItemDesc) * (size_t)b->n, cudaMemcpyHostToDevice));
+        BATCH_CUDA(cudaMemcpy(b->d_items[adjoint ? 1 : 0], b->items.data(), sizeof(ItemDesc) * (size_t)b->n,
+                              cudaMemcpyHostToDevice));
         cudaGraph_t gr = nullptr;
         BATCH_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
         const ctfp_status rs = record(b, adjoint, vols, loss, b->capture);
@@ -387,30 +405,38 @@ struct DevScope {
     }
 };
 
+bool batchable(const ctfp_plan* p)
+{
+    return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_LAYERED;
+}
+
 // Fills the per-call tables from the plans' current state.
 ctfp_status fill_items(ctfp_batch* b)
 {
     for (int s = 0; s < b->n; s++) {
         ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
-        if (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) != SAMPLER_LAYERED)
+        if (!batchable(p))
             return bfail(CTFP_UNSUPPORTED,
                          "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler");
         if (plan_energies(p) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
         ItemDesc& it = b->items[(size_t)s];
         const long long unit0 = it.unit0, units = it.units;
+        const int M = it.M, interp = it.interp;
+        if (plan_materials(p) != M || plan_interp(p) != interp)
+            return bfail(CTFP_INVALID_ARG, "a plan's sampler mode changed after ctfp_batch_create");
         std::memset(&it, 0, sizeof(it));
         it.g = plan_geom(p);
-        it.M = plan_materials(p);
+        it.M = M;
         it.E = plan_energies(p);
-        it.interp = plan_interp(p);
+        it.interp = interp;
         it.mu = plan_mu(p);
         it.W = plan_W(p);
         for (int m = 0; m < it.M; m++) {
             it.ltex[m] = plan_ltex(p, m);
             it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
         }
-        it.tiles_u = (it.g.U + kTU - 1) / kTU;
-        it.tiles_v = (it.g.V + kTV - 1) / kTV;
+        it.patches_u = (it.g.U + kPU - 1) / kPU;
+        it.patches_v = (it.g.V + kPV - 1) / kPV;
         it.unit0 = unit0;
         it.units = units;
     }
@@ -429,25 +455,37 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
     for (int i = 0; i < n_items; i++)
         if (!plans[i]) return bfail(CTFP_INVALID_ARG, "plan is NULL");
     const int dev = plan_device(plans[0]);
-    for (int i = 0; i < n_items; i++)
+    for (int i = 0; i < n_items; i++) {
         if (plan_device(plans[i]) != dev) return bfail(CTFP_INVALID_ARG, "plans must share one device");
+        if (!batchable(plans[i]))
+            return bfail(CTFP_UNSUPPORTED,
+                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler");
+        if (plan_energies(plans[i]) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
+    }
     DevScope ds(dev);
     ctfp_batch* b = new (std::nothrow) ctfp_batch();
     if (!b) return bfail(CTFP_OOM, "host allocation failed");
     b->n = n_items;
     b->device = dev;
     b->plans.assign(plans, plans + n_items);
-    // cost order: rays x samples x materials, largest first; the queue hands
-    // out units in this order (longest-processing-time-first list scheduling)
+    // group by (materials, mode), groups by total cost; within a group cost
+    // order (rays x samples x materials), largest first: the queue hands out
+    // units in this order (longest-processing-time-first list scheduling)
     std::vector<double> cost((size_t)n_items);
     for (int i = 0; i < n_items; i++) {
         const GeomParams& g = plan_geom(plans[i]);
         cost[(size_t)i] = (double)g.U * g.V * g.P * g.K * plan_materials(plans[i]);
     }
+    auto gkey = [&](int i) { return plan_materials(plans[i]) * 4 + plan_interp(plans[i]); };
+    std::vector<double> gcost(32, 0.0);
+    for (int i = 0; i < n_items; i++) gcost[(size_t)gkey(i)] += cost[(size_t)i];
     b->order.resize((size_t)n_items);
     std::iota(b->order.begin(), b->order.end(), 0);
-    std::stable_sort(b->order.begin(), b->order.end(),
-                     [&](int x, int y) { return cost[(size_t)x] > cost[(size_t)y]; });
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+        const int gx = gkey(x), gy = gkey(y);
+        if (gx != gy) return gcost[(size_t)gx] != gcost[(size_t)gy] ? gcost[(size_t)gx] > gcost[(size_t)gy] : gx < gy;
+        return cost[(size_t)x] > cost[(size_t)y];
+    });
     b->items.resize((size_t)n_items);
     b->vox0.resize((size_t)n_items);
     b->gexp_off.assign((size_t)n_items * kMaxM, 0);
@@ -457,12 +495,18 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         ctfp_plan* p = plans[b->order[(size_t)s]];
         const GeomParams& g = plan_geom(p);
         ItemDesc& it = b->items[(size_t)s];
+        it.M = plan_materials(p);
+        it.interp = plan_interp(p);
         it.unit0 = unit;
-        it.units = (long long)((g.U + kTU - 1) / kTU) * ((g.V + kTV - 1) / kTV) * g.P;
+        it.units = (long long)((g.U + kPU - 1) / kPU) * ((g.V + kPV - 1) / kPV) * g.P;
+        if (b->groups.empty() || b->groups.back().M != it.M || b->groups.back().interp != it.interp)
+            b->groups.push_back({it.M, it.interp, s, 0, unit, unit, {0, 0}});
+        b->groups.back().count++;
         unit += it.units;
+        b->groups.back().end = unit;
         b->vox0[(size_t)s] = vox;
         vox += (long long)g.nx * g.ny * g.nz;
-        for (int m = 0; m < plan_materials(p); m++) {
+        for (int m = 0; m < it.M; m++) {
             b->gexp_off[(size_t)s * kMaxM + m] = gexp;
             gexp += expanded_elems(g);
         }
@@ -473,22 +517,26 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
     cudaError_t e = cudaMalloc(&b->d_items[0], sizeof(ItemDesc) * (size_t)n_items);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_items[1], sizeof(ItemDesc) * (size_t)n_items);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_vox0, sizeof(long long) * (size_t)n_items);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(unsigned long long) * b->groups.size());
     if (e == cudaSuccess) e = cudaMalloc(&b->d_gexp, sizeof(float4) * gexp);
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_vox0, b->vox0.data(), sizeof(long long) * (size_t)n_items, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
-    int nsm = 0, per0 = 0, per1 = 0;
+    int nsm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per0, k_batch<false>, kThreads, 0);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_batch<true>, kThreads, 0);
+    for (ctfp_batch::Group& G : b->groups) {
+        for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+            int per = 0;
+            KernelFn fn = k ? kernel_for<true>(G.M, G.interp) : kernel_for<false>(G.M, G.interp);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, 0);
+            G.grid[k] = std::max(1, per) * std::max(1, nsm);
+        }
+    }
     if (e != cudaSuccess) {
         ctfp_batch_destroy(b);
         return bfail(e == cudaErrorMemoryAllocation ? CTFP_OOM : CTFP_CUDA_ERROR,
                      std::string("ctfp_batch_create: ") + cudaGetErrorString(e));
     }
-    b->grid[0] = std::max(1, per0) * std::max(1, nsm);
-    b->grid[1] = std::max(1, per1) * std::max(1, nsm);
     ctfp_status rs = fill_items(b);
     if (rs != CTFP_OK) {
         ctfp_batch_destroy(b);
@@ -566,8 +614,13 @@ ctfp_status ctfp_batch_info(const ctfp_batch* b, int64_t* total_units, int32_t* 
 {
     if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
     if (total_units) *total_units = b->total_units;
-    if (grid_forward) *grid_forward = b->grid[0];
-    if (grid_adjoint) *grid_adjoint = b->grid[1];
+    int g0 = 0, g1 = 0;
+    for (const ctfp_batch::Group& G : b->groups) {
+        g0 = std::max(g0, G.grid[0]);
+        g1 = std::max(g1, G.grid[1]);
+    }
+    if (grid_forward) *grid_forward = g0;
+    if (grid_adjoint) *grid_adjoint = g1;
     return CTFP_OK;
 }
 

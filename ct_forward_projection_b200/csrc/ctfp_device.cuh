@@ -10,6 +10,7 @@
 // reference (CBCTPolyProjGPU.cu:498-517, 557) do not exist.
 #pragma once
 
+#include <climits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -17,7 +18,7 @@ namespace ctfp {
 
 enum { INTERP_TRILINEAR = 0, INTERP_TEXEMU = 1, INTERP_TEXTURE = 2 };
 // Where the software samplers (TRILINEAR, TEXEMU) read their 8 corners.
-enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2 };
+enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2, SAMPLER_BRICK = 3 };
 constexpr int kMaxM = 4;
 
 // Scalar geometry shared by every ray of one problem.
@@ -253,11 +254,12 @@ __device__ __forceinline__ Corner corner_of(double cx, double cy, double cz)
 }
 
 
-// Loads the 8 corners of M volumes for one footprint and interpolates.
-// Corners outside the volume read as 0 (cudaAddressModeBorder, .cu:2200-2202).
-template <int M, int MODE>
-__device__ __forceinline__ void gather_interp(const float* const* __restrict__ vol, int nx, int ny, int nz,
-                                              const Corner& c, float* out)
+// Loads the 8 corners (k = dz*4 + dy*2 + dx) of M volumes for one footprint
+// from the caller's linear volumes.  Corners outside the volume read as 0
+// (cudaAddressModeBorder, CBCTPolyProjGPU.cu:2200-2202).
+template <int M>
+__device__ __forceinline__ void load8_global(const float* const* __restrict__ vol, int nx, int ny, int nz,
+                                             const Corner& c, float (*v)[8])
 {
     const int nxy = nx * ny;
     const bool interior = (unsigned)c.ix < (unsigned)(nx - 1) && (unsigned)c.iy < (unsigned)(ny - 1) &&
@@ -267,9 +269,9 @@ __device__ __forceinline__ void gather_interp(const float* const* __restrict__ v
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const float* __restrict__ q = vol[m] + base;
-            const float v[8] = {__ldg(q), __ldg(q + 1), __ldg(q + nx), __ldg(q + nx + 1),
-                                __ldg(q + nxy), __ldg(q + nxy + 1), __ldg(q + nxy + nx), __ldg(q + nxy + nx + 1)};
-            out[m] = interp8<MODE>(c, v);
+            v[m][0] = __ldg(q); v[m][1] = __ldg(q + 1); v[m][2] = __ldg(q + nx); v[m][3] = __ldg(q + nx + 1);
+            v[m][4] = __ldg(q + nxy); v[m][5] = __ldg(q + nxy + 1);
+            v[m][6] = __ldg(q + nxy + nx); v[m][7] = __ldg(q + nxy + nx + 1);
         }
     } else {
         const bool x0 = (unsigned)c.ix < (unsigned)nx, x1 = (unsigned)(c.ix + 1) < (unsigned)nx;
@@ -278,17 +280,27 @@ __device__ __forceinline__ void gather_interp(const float* const* __restrict__ v
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const float* __restrict__ q = vol[m];
-            const float v[8] = {(x0 && y0 && z0) ? __ldg(q + base) : 0.f,
-                                (x1 && y0 && z0) ? __ldg(q + base + 1) : 0.f,
-                                (x0 && y1 && z0) ? __ldg(q + base + nx) : 0.f,
-                                (x1 && y1 && z0) ? __ldg(q + base + nx + 1) : 0.f,
-                                (x0 && y0 && z1) ? __ldg(q + base + nxy) : 0.f,
-                                (x1 && y0 && z1) ? __ldg(q + base + nxy + 1) : 0.f,
-                                (x0 && y1 && z1) ? __ldg(q + base + nxy + nx) : 0.f,
-                                (x1 && y1 && z1) ? __ldg(q + base + nxy + nx + 1) : 0.f};
-            out[m] = interp8<MODE>(c, v);
+            v[m][0] = (x0 && y0 && z0) ? __ldg(q + base) : 0.f;
+            v[m][1] = (x1 && y0 && z0) ? __ldg(q + base + 1) : 0.f;
+            v[m][2] = (x0 && y1 && z0) ? __ldg(q + base + nx) : 0.f;
+            v[m][3] = (x1 && y1 && z0) ? __ldg(q + base + nx + 1) : 0.f;
+            v[m][4] = (x0 && y0 && z1) ? __ldg(q + base + nxy) : 0.f;
+            v[m][5] = (x1 && y0 && z1) ? __ldg(q + base + nxy + 1) : 0.f;
+            v[m][6] = (x0 && y1 && z1) ? __ldg(q + base + nxy + nx) : 0.f;
+            v[m][7] = (x1 && y1 && z1) ? __ldg(q + base + nxy + nx + 1) : 0.f;
         }
     }
+}
+
+// Loads the 8 corners and interpolates (global sampler).
+template <int M, int MODE>
+__device__ __forceinline__ void gather_interp(const float* const* __restrict__ vol, int nx, int ny, int nz,
+                                              const Corner& c, float* out)
+{
+    float v[M][8];
+    load8_global<M>(vol, nx, ny, nz, c, v);
+#pragma unroll
+    for (int m = 0; m < M; m++) out[m] = interp8<MODE>(c, v[m]);
 }
 
 // Four texels of the 2x2 footprint with lower corner (ix, iy) in one layer
@@ -309,8 +321,8 @@ __device__ __forceinline__ float4 gather_layer(cudaTextureObject_t t, int layer,
 // The 8 corners of M volumes held as layered 2D textures (one layer per z
 // slice): two gathers per material.  Layers outside [0, nz) read as 0 here,
 // since layer indices are clamped, not bordered, by the unit.
-template <int M, int MODE>
-__device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, int nz, const Corner& c, float* out)
+template <int M>
+__device__ __forceinline__ void load8_layered(const cudaTextureObject_t* ltex, int nz, const Corner& c, float (*v)[8])
 {
     const bool z0ok = (unsigned)c.iz < (unsigned)nz, z1ok = (unsigned)(c.iz + 1) < (unsigned)nz;
     const int l0 = z0ok ? c.iz : 0, l1 = z1ok ? c.iz + 1 : 0;
@@ -320,9 +332,19 @@ __device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, 
         float4 b = gather_layer(ltex[m], l1, c.tx, c.ty);
         if (!z0ok) a = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!z1ok) b = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float v[8] = {a.w, a.z, a.x, a.y, b.w, b.z, b.x, b.y};
-        out[m] = interp8<MODE>(c, v);
+        v[m][0] = a.w; v[m][1] = a.z; v[m][2] = a.x; v[m][3] = a.y;
+        v[m][4] = b.w; v[m][5] = b.z; v[m][6] = b.x; v[m][7] = b.y;
     }
+}
+
+// Loads the 8 corners and interpolates (layered sampler).
+template <int M, int MODE>
+__device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, int nz, const Corner& c, float* out)
+{
+    float v[M][8];
+    load8_layered<M>(ltex, nz, c, v);
+#pragma unroll
+    for (int m = 0; m < M; m++) out[m] = interp8<MODE>(c, v[m]);
 }
 
 // Corner-expanded adjoint accumulator.  The 8 transposed weights of a sample
@@ -343,29 +365,53 @@ __device__ __forceinline__ void red_add_v4(float4* p, float a, float b, float c,
                  : "memory");
 }
 
-template <int M, int MODE>
-__device__ __forceinline__ void scatter_expanded(float4* const* __restrict__ gexp, int nx, int ny, int nz,
-                                                 const Corner& c, const float* g)
-{
-    // footprints lie within [-1, n] on every axis: the clipped sample range
-    // only holds samples whose footprint touches the volume
-    float w[8];
-    if (MODE == 1 /* INTERP_TEXEMU */) {
-        texunit_weights(c.qx, c.qy, c.qz, w);
-    } else {
-        const float ux = c.ux, uy = c.uy, uz = c.uz;
-        w[0] = ux * uy * uz; w[1] = c.wx * uy * uz; w[2] = ux * c.wy * uz; w[3] = c.wx * c.wy * uz;
-        w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
-    }
-    if (c.ix < -1 || c.iy < -1 || c.iz < -1 || c.ix >= nx || c.iy >= ny || c.iz >= nz) return;
-    const size_t i0 = exp_index(nx, ny, c.ix, c.iy, c.iz);
-    const size_t i1 = exp_index(nx, ny, c.ix, c.iy, c.iz + 1);
+// Adjoint contributions of consecutive samples that share a footprint, summed
+// in registers and sent with one pair of vector reductions per material when
+// the footprint changes (and at the end of the ray): the same sums as one
+// reduction pair per sample, in fewer L2 atomics.
+template <int M>
+struct ScatterRun {
+    int ix = INT_MIN, iy = 0, iz = 0;
+    float a[M][8];
+    __device__ __forceinline__ void flush(float4* const* __restrict__ gexp, int nx, int ny, int nz)
+    {
+        if (ix == INT_MIN) return;
+        if (ix < -1 || iy < -1 || iz < -1 || ix >= nx || iy >= ny || iz >= nz) return;
+        const size_t i0 = exp_index(nx, ny, ix, iy, iz);
+        const size_t i1 = exp_index(nx, ny, ix, iy, iz + 1);
 #pragma unroll
-    for (int m = 0; m < M; m++) {
-        red_add_v4(gexp[m] + i0, w[0] * g[m], w[1] * g[m], w[2] * g[m], w[3] * g[m]);
-        red_add_v4(gexp[m] + i1, w[4] * g[m], w[5] * g[m], w[6] * g[m], w[7] * g[m]);
+        for (int m = 0; m < M; m++) {
+            red_add_v4(gexp[m] + i0, a[m][0], a[m][1], a[m][2], a[m][3]);
+            red_add_v4(gexp[m] + i1, a[m][4], a[m][5], a[m][6], a[m][7]);
+        }
     }
-}
+    template <int MODE>
+    __device__ __forceinline__ void add(float4* const* __restrict__ gexp, int nx, int ny, int nz, const Corner& c,
+                                        const float* g)
+    {
+        float w[8];
+        if (MODE == 1 /* INTERP_TEXEMU */) {
+            texunit_weights(c.qx, c.qy, c.qz, w);
+        } else {
+            const float ux = c.ux, uy = c.uy, uz = c.uz;
+            w[0] = ux * uy * uz; w[1] = c.wx * uy * uz; w[2] = ux * c.wy * uz; w[3] = c.wx * c.wy * uz;
+            w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
+        }
+        if (c.ix != ix || c.iy != iy || c.iz != iz) {
+            flush(gexp, nx, ny, nz);
+            ix = c.ix; iy = c.iy; iz = c.iz;
+#pragma unroll
+            for (int m = 0; m < M; m++)
+#pragma unroll
+                for (int k = 0; k < 8; k++) a[m][k] = w[k] * g[m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < M; m++)
+#pragma unroll
+                for (int k = 0; k < 8; k++) a[m][k] = fmaf(w[k], g[m], a[m][k]);
+        }
+    }
+};
 
 // Compensated (Kahan) accumulation, FP32.
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x)

@@ -15,11 +15,22 @@ namespace ctfp {
 
 namespace {
 
-template <int M, int MODE, int SAMPLER>
-__device__ __forceinline__ void sample_corner(const MarchParams& prm, const Corner& c, float* val)
+template <int M, int SAMPLER>
+__device__ __forceinline__ void load_corners(const MarchParams& prm, const Corner& c, float (*v)[8])
 {
-    if (SAMPLER == SAMPLER_LAYERED) gather4_interp<M, MODE>(prm.ltex, prm.g.nz, c, val);
-    else gather_interp<M, MODE>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, val);
+    if (SAMPLER == SAMPLER_LAYERED) load8_layered<M>(prm.ltex, prm.g.nz, c, v);
+    else load8_global<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, v);
+}
+
+// One sample of a software-interpolated march: fetch the footprint,
+// interpolate, accumulate.
+template <int M, int MODE, int SAMPLER>
+__device__ __forceinline__ void sample_acc(const MarchParams& prm, const Corner& c, float* acc, float* cmp)
+{
+    float v[M][8];
+    load_corners<M, SAMPLER>(prm, c, v);
+#pragma unroll
+    for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], interp8<MODE>(c, v[m]));
 }
 
 // L_m for one ray, compensated FP32 sum times dx.  TRILINEAR samples at FP64
@@ -35,28 +46,22 @@ __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, 
 #pragma unroll 2
         for (int i = s.i0; i < s.i1; i++) {
             const double t = (double)i;
-            float val[M];
-            sample_corner<M, MODE, SAMPLER>(
-                prm, corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az)), val);
-#pragma unroll
-            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+            sample_acc<M, MODE, SAMPLER>(
+                prm, corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az)), acc, cmp);
         }
-    } else {
+    } else if (MODE == INTERP_TEXTURE) {
+        // the reference's own fetch: tex3D on a border/linear texture
         const RayRef32 r = ray_ref32(prm.g, p, v, u);
 #pragma unroll 2
         for (int i = s.i0; i < s.i1; i++) {
             const float3 x = ref32_coords(prm.g, r, i);
-            float val[M];
-            if (MODE == INTERP_TEXTURE) {
-                // the reference's own fetch: tex3D on a border/linear texture
 #pragma unroll
-                for (int m = 0; m < M; m++) val[m] = tex3D<float>(prm.tex[m], x.x, x.y, x.z);
-            } else {
-                sample_corner<M, MODE, SAMPLER>(prm, corner_tex(x), val);
-            }
-#pragma unroll
-            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], val[m]);
+            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(prm.tex[m], x.x, x.y, x.z));
         }
+    } else {
+        const RayRef32 r = ray_ref32(prm.g, p, v, u);
+#pragma unroll 2
+        for (int i = s.i0; i < s.i1; i++) sample_acc<M, MODE, SAMPLER>(prm, corner_tex(ref32_coords(prm.g, r, i)), acc, cmp);
     }
 #pragma unroll
     for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
@@ -223,19 +228,21 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
         for (int m = 0; m < M; m++) any |= (g[m] != 0.f);
         if (!any) continue;
         const RaySeg s = ray_segment(prm.g, p, v, u);
+        ScatterRun<M> run;
         if (MODE == INTERP_TRILINEAR) {
             for (int i = s.i0; i < s.i1; i++) {
                 const double t = (double)i;
                 const Corner c = corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
-                scatter_expanded<M, INTERP_TRILINEAR>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
+                run.template add<INTERP_TRILINEAR>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
             }
         } else {
             // transpose of the texture-unit sampler at the reference's FP32 coordinates
             const RayRef32 r = ray_ref32(prm.g, p, v, u);
             for (int i = s.i0; i < s.i1; i++)
-                scatter_expanded<M, INTERP_TEXEMU>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz,
-                                                   corner_tex(ref32_coords(prm.g, r, i)), g);
+                run.template add<INTERP_TEXEMU>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz,
+                                                corner_tex(ref32_coords(prm.g, r, i)), g);
         }
+        run.flush(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz);
     }
 }
 
@@ -336,6 +343,175 @@ __global__ void k_count_support(const GeomParams g, unsigned long long* out)
     if ((threadIdx.x & 31) == 0) atomicAdd(out, n);
 }
 
+// ---------------------------------------------------------------------------
+// Brick sampler: the CTA stages, for every segment of kBS consecutive samples,
+// the box of voxels its ray bundle crosses in shared memory, and each sample
+// reads its 8 corners from there (LDS) instead of through the texture unit.
+// Rays of one CTA step through the same sample indices, so at any index their
+// samples lie on a small patch: kBU x kBV rays about one voxel apart, swept
+// kBS/2 voxels along the rays per segment.  The box origin and fit are
+// computed per segment from the rays' first and last footprints (FP64
+// coordinates are affine in the sample index, so their floors are monotone;
+// the FP32 compat coordinates get a one-voxel margin).  A segment whose box
+// does not fit, and any sample outside the box, reads the caller's volume
+// instead, so the result never depends on the fit.
+constexpr int kBU = 8, kBV = 16;             // rays per CTA: u x v
+constexpr int kBX = 16, kBY = 16, kBZ = 20;  // box, voxels
+constexpr int kBXp = 17;                     // row pitch (floats)
+constexpr int kBZp = 296;                    // slice pitch: 17 * 16 + 24 = 8 (mod 32 banks)
+constexpr int kBS = 16;                      // samples per segment
+constexpr int kBoxFloats = kBZp * kBZ;       // one material's box
+
+template <int MODE>
+__device__ __forceinline__ Corner corner_at(const MarchParams& prm, const RaySeg& s, const RayRef32& r, int i)
+{
+    if (MODE == INTERP_TRILINEAR) {
+        const double t = (double)i;
+        return corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+    }
+    return corner_tex(ref32_coords(prm.g, r, i));
+}
+
+template <int M, int MODE, bool SPECTRAL, int MINB>
+__global__ void __launch_bounds__(kBU * kBV, MINB) k_forward_brick(const MarchParams prm)
+{
+    extern __shared__ float smem[];
+    float* s_box = smem;                   // [M][kBZ][kBY][kBXp] (slices kBZp apart)
+    float* s_mu = smem + M * kBoxFloats;   // [E][M]
+    __shared__ int s_red[8];
+    if (SPECTRAL) load_mu(s_mu, prm.mu, prm.E * M);
+    const int tid = threadIdx.y * kBU + threadIdx.x;
+    const int u = blockIdx.x * kBU + threadIdx.x;
+    const int v = blockIdx.y * kBV + threadIdx.y;
+    const bool live = u < prm.g.U && v < prm.g.V;
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t pix = (int64_t)v * prm.g.U + u;
+    const int pend = prm.view0 + prm.n_views;
+    constexpr int margin = MODE == INTERP_TRILINEAR ? 0 : 1;
+    for (int k = 0; k < prm.views_per_cta; k++) {
+        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        if (p >= pend) break;
+        RaySeg s;
+        s.i0 = s.i1 = 0;
+        if (live) s = ray_segment(prm.g, p, v, u);
+        RayRef32 r;
+        if (MODE != INTERP_TRILINEAR && live) r = ray_ref32(prm.g, p, v, u);
+        if (tid == 0) {
+            s_red[0] = INT_MAX;
+            s_red[1] = INT_MIN;
+        }
+        __syncthreads();
+        if (s.i1 > s.i0) {
+            atomicMin(&s_red[0], s.i0);
+            atomicMax(&s_red[1], s.i1);
+        }
+        __syncthreads();
+        const int I0 = s_red[0], I1 = s_red[1];
+        __syncthreads();
+        float acc[M], cmp[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+        for (int seg = I0; seg < I1; seg += kBS) {
+            const int a0 = max(seg, s.i0), a1 = min(min(seg + kBS, I1), s.i1);
+            if (tid == 0) {
+                s_red[0] = s_red[1] = s_red[2] = INT_MAX;
+                s_red[3] = s_red[4] = s_red[5] = INT_MIN;
+            }
+            __syncthreads();
+            if (a0 < a1) {
+                const Corner c0 = corner_at<MODE>(prm, s, r, a0), c1 = corner_at<MODE>(prm, s, r, a1 - 1);
+                atomicMin(&s_red[0], min(c0.ix, c1.ix) - margin);
+                atomicMin(&s_red[1], min(c0.iy, c1.iy) - margin);
+                atomicMin(&s_red[2], min(c0.iz, c1.iz) - margin);
+                atomicMax(&s_red[3], max(c0.ix, c1.ix) + margin);
+                atomicMax(&s_red[4], max(c0.iy, c1.iy) + margin);
+                atomicMax(&s_red[5], max(c0.iz, c1.iz) + margin);
+            }
+            __syncthreads();
+            const int ox = s_red[0], oy = s_red[1], oz = s_red[2];
+            const bool fits = s_red[3] >= ox && s_red[3] + 1 - ox < kBX && s_red[4] + 1 - oy < kBY &&
+                              s_red[5] + 1 - oz < kBZ;
+            if (fits) {
+                // stage the box; voxels outside the volume read as 0 (border)
+                const int nx = prm.g.nx, ny = prm.g.ny, nz = prm.g.nz;
+                for (int idx = tid; idx < kBX * kBY * kBZ; idx += kBU * kBV) {
+                    const int x = idx % kBX, y = (idx / kBX) % kBY, z = idx / (kBX * kBY);
+                    const int gx = ox + x, gy = oy + y, gz = oz + z;
+                    const bool in = (unsigned)gx < (unsigned)nx && (unsigned)gy < (unsigned)ny &&
+                                    (unsigned)gz < (unsigned)nz;
+                    const int64_t off = ((int64_t)gz * ny + gy) * nx + gx;
+                    const int so = z * kBZp + y * kBXp + x;
+#pragma unroll
+                    for (int m = 0; m < M; m++) s_box[m * kBoxFloats + so] = in ? __ldg(prm.vol[m] + off) : 0.f;
+                }
+            }
+            __syncthreads();
+            for (int i = a0; i < a1; i++) {
+                const Corner c = corner_at<MODE>(prm, s, r, i);
+                const int bx = c.ix - ox, by = c.iy - oy, bz = c.iz - oz;
+                float cv[M][8];
+                if (fits && (unsigned)bx < (unsigned)(kBX - 1) && (unsigned)by < (unsigned)(kBY - 1) &&
+                    (unsigned)bz < (unsigned)(kBZ - 1)) {
+                    const int b = bz * kBZp + by * kBXp + bx;
+#pragma unroll
+                    for (int m = 0; m < M; m++) {
+                        const float* q = s_box + m * kBoxFloats + b;
+                        cv[m][0] = q[0]; cv[m][1] = q[1]; cv[m][2] = q[kBXp]; cv[m][3] = q[kBXp + 1];
+                        cv[m][4] = q[kBZp]; cv[m][5] = q[kBZp + 1]; cv[m][6] = q[kBZp + kBXp];
+                        cv[m][7] = q[kBZp + kBXp + 1];
+                    }
+                } else {
+                    load8_global<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, cv);
+                }
+#pragma unroll
+                for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], interp8<MODE>(c, cv[m]));
+            }
+            __syncthreads();
+        }
+        if (!live) continue;
+        float L[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
+        const int64_t ray = (int64_t)p * npix + pix;
+        if (prm.L) store_L<M>(prm.L, ray, L);
+        if (SPECTRAL) {
+            float I, A;
+            spectral<M>(s_mu, prm.E, prm.W, pix, npix, L, I, A);
+            if (prm.I) prm.I[ray] = I;
+            if (prm.IAbs) prm.IAbs[ray] = A;
+        }
+    }
+}
+
+template <int M, int MODE, bool SPEC>
+cudaError_t brick_launch(const MarchParams& prm, dim3 grid, size_t smem, cudaStream_t st)
+{
+    // the dynamic shared-memory opt-in is per device
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(attr_set >> dev & 1ull)) {
+        cudaError_t e = cudaFuncSetAttribute(k_forward_brick<M, MODE, SPEC, 4>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set |= 1ull << dev;
+    }
+    k_forward_brick<M, MODE, SPEC, 4><<<grid, dim3(kBU, kBV), smem, st>>>(prm);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t brick_dispatch(const MarchParams& prm, int interp, bool spec, dim3 grid, size_t smem, cudaStream_t st)
+{
+    if (interp == INTERP_TRILINEAR)
+        return spec ? brick_launch<M, INTERP_TRILINEAR, true>(prm, grid, smem, st)
+                    : brick_launch<M, INTERP_TRILINEAR, false>(prm, grid, smem, st);
+    if (interp == INTERP_TEXEMU)
+        return spec ? brick_launch<M, INTERP_TEXEMU, true>(prm, grid, smem, st)
+                    : brick_launch<M, INTERP_TEXEMU, false>(prm, grid, smem, st);
+    return cudaErrorInvalidValue;
+}
+
 template <int M, int MODE, int SAMPLER, int MINB>
 cudaError_t fwd_launch(const MarchParams& prm, bool spec, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
 {
@@ -401,6 +577,19 @@ cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sam
 {
     MarchParams prm = prm_in;
     prm.views_per_cta = ls.views_per_cta;
+    if (sampler == SAMPLER_BRICK && interp != INTERP_TEXTURE) {
+        const dim3 grid((prm.g.U + kBU - 1) / kBU, (prm.g.V + kBV - 1) / kBV,
+                        (prm.n_views + ls.views_per_cta - 1) / ls.views_per_cta);
+        if (grid.z == 0) return cudaSuccess;
+        const size_t smem = sizeof(float) * ((size_t)M * kBoxFloats + (do_spectral ? (size_t)prm.E * M : 0));
+        switch (M) {
+            case 1: return brick_dispatch<1>(prm, interp, do_spectral, grid, smem, st);
+            case 2: return brick_dispatch<2>(prm, interp, do_spectral, grid, smem, st);
+            case 3: return brick_dispatch<3>(prm, interp, do_spectral, grid, smem, st);
+            case 4: return brick_dispatch<4>(prm, interp, do_spectral, grid, smem, st);
+        }
+        return cudaErrorInvalidValue;
+    }
     const dim3 block(ls.tile_u, ls.tile_v), grid = march_grid(prm, ls);
     const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;

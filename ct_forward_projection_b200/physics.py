@@ -266,3 +266,32 @@ def label_phantom(w: Workload, seed_offset: int = 0) -> np.ndarray:
     for m, v in enumerate(maps):
         lab[v > 0] = m + 1
     return lab.numpy()
+
+
+def batch_workloads(n: int = 48, seed: int = 4000) -> list:
+    """The uneven batch: n seeded problems with volumes from 64^3 to
+    320 x 320 x 200 (1-3 materials), SOD 900-1100 / SDD 1300-1600 mm, 30-720
+    views, detectors 128^2 to 768 x 512, spectra 60-140 kVp in 1-keV bins from
+    20 keV (41-121 bins).  The detector pitch makes the field of view cover the
+    volume's diagonal; half the problems carry a focused grid."""
+    rng = np.random.RandomState(seed)
+    mats = {1: ["water"], 2: ["soft_tissue", "bone"], 3: ["soft_tissue", "bone", "iodine"]}
+    out = []
+    for k in range(n):
+        nxy = int(rng.randint(64, 321))
+        nz = int(rng.randint(64, 201))
+        M = int(rng.randint(1, 4))
+        views = int(rng.randint(30, 721))
+        U = int(rng.randint(128, 769))
+        V = int(rng.randint(128, 513))
+        sod = float(rng.uniform(900.0, 1100.0))
+        sdd = float(rng.uniform(1300.0, 1600.0))
+        kvp = int(rng.randint(60, 141))
+        vox = float(rng.uniform(0.4, 1.0))
+        L = nxy * vox
+        pitch = 1.5 * L * sdd / sod / U
+        grid = GridSpec(50, 200, 2.0, sdd) if rng.uniform() < 0.5 else None
+        g = _geom((nxy, nxy, nz), (L, L, nz * vox), views, U, V, pitch, sod=sod, sdd=sdd)
+        out.append(Workload(f"batch_{k:02d}", g, mats[M], kvp, 20, 2.0, grid, grid_layout=2, scint_mm=0.6,
+                            seed=seed + 1 + k))
+    return out

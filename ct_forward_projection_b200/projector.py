@@ -113,8 +113,10 @@ class Projector:
         self.interp = interp
 
     def set_sampler(self, sampler: str) -> None:
-        """'global' (linear volumes through L1) or 'layered' (texture gathers)."""
-        call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED}[sampler])
+        """'global' (linear volumes through L1), 'layered' (texture gathers) or
+        'brick' (per-bundle voxel boxes in shared memory)."""
+        call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED,
+                                                 "brick": capi.SAMPLER_BRICK}[sampler])
 
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)

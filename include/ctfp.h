@@ -88,7 +88,11 @@ typedef enum ctfp_sampler {
     /* plan-owned layered 2D textures, one layer per z slice: two texture
      * gathers (tld4) return the 8 corners; weights stay in software.  Default;
      * needs pNumZ <= 2048. */
-    CTFP_SAMPLER_LAYERED = 2
+    CTFP_SAMPLER_LAYERED = 2,
+    /* the caller's linear volumes staged per ray bundle in shared memory: each
+     * CTA (8 x 16 rays, one view at a time) copies the voxel box its rays cross
+     * in the next 16 samples and reads corners from there */
+    CTFP_SAMPLER_BRICK = 3
 } ctfp_sampler;
 
 /* Grid transmission table layout for ctfp_set_spectral_tables. */
@@ -218,15 +222,17 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
 
 /* ---- batched form -------------------------------------------------------------
  * No counterpart in the reference, which simulates one phantom per process run
- * (main.cpp:4-8).  A batch holds n_items plans (own geometry, materials,
- * spectral tables; one device) and runs all of them in ONE persistent launch
- * over a device work queue: a work unit is one view x one 16 x 8 detector
- * tile; items are queued largest first (rays x samples x materials), each CTA
- * takes the next unit from an atomic counter.  A call is recorded once as a
- * CUDA graph (volume uploads, queue reset, kernel, fold) and replayed, in the
- * order of the stream passed, while the item pointers and the plans' tables
- * stay the same; a change re-records it (one host synchronisation).  The batch
- * uploads into the plans' own texture arrays: do not run a batch and its plans
+ * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
+ * spectral tables; one device) and runs them with persistent kernels over a
+ * device work queue: a work unit is one view x one 8 x 4 detector patch (the
+ * 32 rays of one warp); items are grouped by material count and sampler mode
+ * (one kernel per group, each with its own register budget) and queued
+ * largest first (rays x samples x materials); every warp takes the next unit
+ * from an atomic counter.  A call is recorded once as a CUDA graph (volume
+ * uploads, queue reset, kernels, fold) and replayed, in the order of the
+ * stream passed, while the item pointers and the plans' tables stay the same;
+ * a change re-records it (one host synchronisation).  The batch uploads into
+ * the plans' own texture arrays: do not run a batch and its plans
  * concurrently.
  *
  * Items must use CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered

@@ -48,7 +48,7 @@ GEOMS = [
 ]
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 3, 4])
 def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
@@ -61,7 +61,7 @@ def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
     assert rel_err_scaled(L, Lref) < RTOL_TRI
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 4])
 def test_forward_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
@@ -102,7 +102,7 @@ def test_forward_grid_layouts_and_no_response(cuda_ok, layout):
     assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TRI
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
 @pytest.mark.parametrize("M", [1, 2, 3])
 def test_forward_texemu_vs_oracle(cuda_ok, M, sampler):
     d = small_geometry(n=20, views=5, U=24, V=14)
@@ -223,3 +223,21 @@ def test_rays_missing_volume_are_zero(cuda_ok):
     ref = O.line_integrals(d, vols).reshape(-1)
     assert np.array_equal(L == 0, ref == 0)
     assert rel_err_scaled(L, ref) < RTOL_TRI
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("pitch", [None, 9.0])
+def test_brick_sampler_equals_layered(cuda_ok, mode, pitch):
+    # same corner values, weights and summation order: identical results,
+    # whether the bundle's boxes fit (default pitch) or not (rays many voxels
+    # apart: every segment reads the caller's volume instead)
+    d = small_geometry(n=(40, 36, 30), views=5, U=37, V=35, pitch=pitch)
+    vols = random_volumes(d, 3, 12)
+    S, mu, G, D = spectral_setup(d, 3, 6, 2)
+    with Projector(d, 3, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        a = pr.forward(to_dev(vols), want_L=True)
+        pr.set_sampler("brick")
+        b = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    assert torch.equal(a["L"], b["L"]) and torch.equal(a["I"], b["I"]) and torch.equal(a["IAbsorb"], b["IAbsorb"])
