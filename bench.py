@@ -36,6 +36,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) per full forward launch, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 36-view case of the
+# same problem, scaled by views (traffic grows with the views marched); see
+# profiles/k_forward_layered_poly_grid_256.md.
+TRAFFIC_PER_LAUNCH = {}
 BYTES_PER_VOXEL_SAMPLE = 32  # 8 FP32 corners, the reuse-free trilinear footprint
 
 
@@ -281,11 +286,21 @@ def main():
     nominal_vs = M * rays * int(pr.info["intNum"])
     peak, peak_kind = measured_peak_hbm()
     achieved = vs_launch * BYTES_PER_VOXEL_SAMPLE / (ms / 1e3) / 1e9
+    vs_rate = vs_launch / (ms / 1e3)
+    from ct_forward_projection_b200.projector import sampler_peak
+    tex_peak = sampler_peak(local, "tex3d" if args.interp == "texture" else "layered")
+    traffic = TRAFFIC_PER_LAUNCH.get((w.name, args.interp))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_source": peak_kind,
-                "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_launch / (ms / 1e3),
+                "traffic": traffic, "peak_source": peak_kind,
+                "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_rate,
                 "nominal_voxel_samples_per_launch": nominal_vs,
-                "note": "achieved = 32 B x support voxel-samples / kernel time; traffic from ncu in profiles/"}
+                "texture": {"peak_voxel_samples_per_s": tex_peak, "achieved_voxel_samples_per_s": vs_rate,
+                            "frac": vs_rate / tex_peak, "binding": True,
+                            "peak_source": "ctfp_sampler_peak, measured in this run"},
+                "roof_min_hbm32_tex": min(peak * 1e9 / BYTES_PER_VOXEL_SAMPLE, tex_peak),
+                "note": ("achieved = 32 B (reuse-free 8-corner footprint) x support voxel-samples / kernel time; "
+                         "the texture cache serves most corners, so DRAM traffic (ncu) is far below that and the "
+                         "binding ceiling is the texture path (texture.frac)")}
 
     # ---------------- end to end through ctfp_forward_host (e2e) ------------
     e2e = None

@@ -86,6 +86,7 @@ _SIGNATURES = {
     "ctfp_labels_to_density": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, _P]),
     "ctfp_forward_noalloc": (C.c_int, [C.POINTER(Geometry), C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
                                        _P, C.c_float, _P, _P, _P, _P, _P]),
+    "ctfp_sampler_peak": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "ctfp_plan_autotune": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.POINTER(LaunchShape), _P]),
     "ctfp_batch_create": (C.c_int, [C.c_int32, _P, C.POINTER(_P)]),
     "ctfp_batch_destroy": (C.c_int, [_P]),

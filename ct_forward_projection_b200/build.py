@@ -28,7 +28,7 @@ LIB = os.path.join(PKG, "libctfp.so")
 COMPAT_LIB = os.path.join(PKG, "libctfp_compat.so")
 CLI = os.path.join(PKG, "ctfp_forward_projection")
 
-CU_SOURCES = ["ctfp_api.cu", "ctfp_kernels.cu", "ctfp_batch.cu", "ctfp_autotune.cu", "ctfp_tables.cu", "ctfp_noalloc.cu"]
+CU_SOURCES = ["ctfp_api.cu", "ctfp_kernels.cu", "ctfp_batch.cu", "ctfp_autotune.cu", "ctfp_tables.cu", "ctfp_noalloc.cu", "ctfp_diag.cu"]
 
 
 def _run(cmd: list[str]) -> None:

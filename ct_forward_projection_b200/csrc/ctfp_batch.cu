@@ -3,13 +3,13 @@
 // device work queue, the whole call replayed as one CUDA graph.  No reference
 // counterpart.
 //
-// Work unit = (item, view, 8 x 4 pixel patch): the 32 rays of one warp.  Items
-// are grouped by material count and sampler mode (one kernel instantiation
-// each, so every group runs with the registers its own march needs); within a
-// group they are queued largest first (rays x samples x materials), and every
-// warp takes the next unit from the group's counter (atomicAdd, no waits, no
-// block barriers), so long problems start early, short ones fill the tail,
-// and a warp whose rays were short moves on at once.
+// Work unit = (item, view, 16 x 8 pixel tile): the 128 rays of one CTA, whose
+// neighbouring rays share texture-cache lines.  Items are grouped by material
+// count and sampler mode (one kernel instantiation each, so every group runs
+// with the registers its own march needs); within a group they are queued
+// largest first (rays x samples x materials), and every CTA takes the next
+// unit from the group's counter (atomicAdd, no waits), so long problems start
+// early and short ones fill the tail.
 //
 // Two kinds of call: the forward (march + spectral epilogue, optional
 // checkpoint) and the fused forward + loss + adjoint, which for every ray
@@ -45,7 +45,7 @@ using namespace ctfp;
 
 namespace {
 
-constexpr int kPU = 8, kPV = 4;       // rays of one unit (one warp): u x v
+constexpr int kTU = 16, kTV = 8;      // rays of one unit (one CTA): u x v
 constexpr int kWarps = 4, kThreads = 32 * kWarps;
 
 // One item as the persistent kernels see it.  The pointer fields are refreshed
@@ -56,7 +56,7 @@ struct ItemDesc {
     const float* mu;   // [E][M]
     const float* W;    // [E][V][U]
     int M, E, interp;
-    int patches_u, patches_v;
+    int tiles_u, tiles_v;
     long long unit0;   // first unit of this item in the batch's numbering
     long long units;
     // per call
@@ -199,34 +199,57 @@ struct BatchBudget {
 template <int M, int MODE, bool ADJOINT>
 __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M>::minb) k_batch(const GroupArgs a)
 {
-    __shared__ float s_mu_all[kWarps][CTFP_MAX_ENERGIES * M];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* s_mu = s_mu_all[warp];
+    __shared__ float s_mu[CTFP_MAX_ENERGIES * M];
+    __shared__ long long s_unit;
+    __shared__ float s_loss[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int cached = -1;
     for (;;) {
-        long long unit = 0;
-        if (lane == 0) unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
-        unit = __shfl_sync(0xffffffffu, unit, 0);
+        __syncthreads();  // the previous unit is done with s_mu, s_loss, s_unit
+        if (threadIdx.x == 0) s_unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
+        __syncthreads();
+        const long long unit = s_unit;
         if (unit >= a.end) break;
         const int k = find_item(a, unit);
         const ItemDesc& it = a.items[k];
         if (k != cached) {
-            __syncwarp();
-            for (int j = lane; j < it.E * M; j += 32) s_mu[j] = it.mu[j];
-            __syncwarp();
+            for (int j = threadIdx.x; j < it.E * M; j += kThreads) s_mu[j] = it.mu[j];
             cached = k;
+            __syncthreads();
         }
+        // unit order within an item.  Forward: view, then tile row, then tile
+        // column.  Adjoint: tile row, then view, then tile column, so that the
+        // CTAs resident at any time work on one band of detector rows over
+        // many views: those rays cross a thin z-slab of the volume, whose
+        // accumulator cells then stay in L2.
         const long long local = unit - it.unit0;
-        const int patches = it.patches_u * it.patches_v;
-        const int p = (int)(local / patches);
-        const int patch = (int)(local % patches);
-        const int u = (patch % it.patches_u) * kPU + (lane % kPU);
-        const int v = (patch / it.patches_u) * kPV + (lane / kPU);
+        int p, tu, tv;
+        if (ADJOINT) {
+            const long long band_units = (long long)it.g.P * it.tiles_u;
+            tv = (int)(local / band_units);
+            const int rem = (int)(local % band_units);
+            p = rem / it.tiles_u;
+            tu = rem % it.tiles_u;
+        } else {
+            const int tiles = it.tiles_u * it.tiles_v;
+            p = (int)(local / tiles);
+            const int t = (int)(local % tiles);
+            tv = t / it.tiles_u;
+            tu = t % it.tiles_u;
+        }
+        const int u = tu * kTU + (threadIdx.x % kTU);
+        const int v = tv * kTV + (threadIdx.x / kTU);
         float loss = 0.f;
         if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT>(it, s_mu, p, v, u);
         if (ADJOINT && it.loss) {
             for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
-            if (lane == 0) atomicAdd(it.loss, loss);
+            if (lane == 0) s_loss[warp] = loss;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float t = 0.f;
+                for (int w = 0; w < kWarps; w++) t += s_loss[w];
+                atomicAdd(it.loss, t);
+            }
         }
     }
 }
@@ -435,8 +458,8 @@ ctfp_status fill_items(ctfp_batch* b)
             it.ltex[m] = plan_ltex(p, m);
             it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
         }
-        it.patches_u = (it.g.U + kPU - 1) / kPU;
-        it.patches_v = (it.g.V + kPV - 1) / kPV;
+        it.tiles_u = (it.g.U + kTU - 1) / kTU;
+        it.tiles_v = (it.g.V + kTV - 1) / kTV;
         it.unit0 = unit0;
         it.units = units;
     }
@@ -498,7 +521,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         it.M = plan_materials(p);
         it.interp = plan_interp(p);
         it.unit0 = unit;
-        it.units = (long long)((g.U + kPU - 1) / kPU) * ((g.V + kPV - 1) / kPV) * g.P;
+        it.units = (long long)((g.U + kTU - 1) / kTU) * ((g.V + kTV - 1) / kTV) * g.P;
         if (b->groups.empty() || b->groups.back().M != it.M || b->groups.back().interp != it.interp)
             b->groups.push_back({it.M, it.interp, s, 0, unit, unit, {0, 0}});
         b->groups.back().count++;

@@ -9,6 +9,8 @@
 // all energies (sum_m mu[e][m] * L_m equals the reference's per-energy
 // mu_E-volume integral because trilinear interpolation is linear in the voxel
 // values), and the energy sum runs on the device in compensated FP32.
+#include <algorithm>
+
 #include "ctfp_kernels.cuh"
 
 namespace ctfp {
@@ -184,21 +186,28 @@ __global__ void __launch_bounds__(256) k_spectral_from_L(const MarchParams prm)
 }
 
 // Adjoint: spectral-weight recompute from the checkpoint, then the matched
-// ray march scattering the transposed trilinear weights with FP32 atomics.
-// FROM_GL: the input is dLoss/dL directly (transpose of the line integrals).
+// ray march scattering the transposed trilinear weights with vector
+// reductions.  FROM_GL: the input is dLoss/dL directly (transpose of the line
+// integrals).
+//
+// Grid: x = pixel tiles along u, y = view groups, z = pixel tiles along v, so
+// that the CTAs resident at any time cover one band of detector rows for many
+// views.  The rays of a row band cross a thin z-slab of the volume (the cone
+// angle is small), so the accumulator cells they reduce into stay in L2; with
+// views outermost every view would sweep the whole accumulator through DRAM.
 template <int M, int MODE, bool FROM_GL>
 __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
 {
     extern __shared__ float s_mu[];
     if (!FROM_GL) load_mu(s_mu, prm.mu, prm.E * M);
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = blockIdx.y * blockDim.y + threadIdx.y;
+    const int v = blockIdx.z * blockDim.y + threadIdx.y;
     if (u >= prm.g.U || v >= prm.g.V) return;
     const int64_t npix = (int64_t)prm.g.U * prm.g.V;
     const int64_t pix = (int64_t)v * prm.g.U + u;
     const int pend = prm.view0 + prm.n_views;
     for (int k = 0; k < prm.views_per_cta; k++) {
-        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        const int p = prm.view0 + blockIdx.y * prm.views_per_cta + k;
         if (p >= pend) break;
         const int64_t ray = (int64_t)p * npix + pix;
         float g[M];
@@ -623,18 +632,30 @@ cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t s
 cudaError_t launch_backward(const MarchParams& prm_in, int M, int interp, bool from_gL, const LaunchShape& ls,
                             cudaStream_t st)
 {
-    MarchParams prm = prm_in;
-    prm.views_per_cta = ls.views_per_cta;
-    const dim3 block(ls.tile_u, ls.tile_v), grid = march_grid(prm, ls);
-    const size_t smem = sizeof(float) * (size_t)prm.E * M;
-    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
-    switch (M) {
-        case 1: return bwd_dispatch<1>(prm, interp, from_gL, grid, block, smem, st);
-        case 2: return bwd_dispatch<2>(prm, interp, from_gL, grid, block, smem, st);
-        case 3: return bwd_dispatch<3>(prm, interp, from_gL, grid, block, smem, st);
-        case 4: return bwd_dispatch<4>(prm, interp, from_gL, grid, block, smem, st);
+    const dim3 block(ls.tile_u, ls.tile_v);
+    const size_t smem = sizeof(float) * (size_t)prm_in.E * M;
+    // row bands outermost (grid.z), views in grid.y: at most 65535 view
+    // groups per launch
+    const int vpc = ls.views_per_cta;
+    const int max_views = 65535 * vpc;
+    for (int v0 = 0; v0 < prm_in.n_views; v0 += max_views) {
+        MarchParams prm = prm_in;
+        prm.views_per_cta = vpc;
+        prm.view0 = prm_in.view0 + v0;
+        prm.n_views = std::min(max_views, prm_in.n_views - v0);
+        const dim3 grid((prm.g.U + ls.tile_u - 1) / ls.tile_u, (prm.n_views + vpc - 1) / vpc,
+                        (prm.g.V + ls.tile_v - 1) / ls.tile_v);
+        if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
+        cudaError_t e = cudaErrorInvalidValue;
+        switch (M) {
+            case 1: e = bwd_dispatch<1>(prm, interp, from_gL, grid, block, smem, st); break;
+            case 2: e = bwd_dispatch<2>(prm, interp, from_gL, grid, block, smem, st); break;
+            case 3: e = bwd_dispatch<3>(prm, interp, from_gL, grid, block, smem, st); break;
+            case 4: e = bwd_dispatch<4>(prm, interp, from_gL, grid, block, smem, st); break;
+        }
+        if (e != cudaSuccess) return e;
     }
-    return cudaErrorInvalidValue;
+    return cudaSuccess;
 }
 
 size_t expanded_elems(const GeomParams& g) { return (size_t)(g.nz + 2) * (size_t)(g.ny + 1) * (size_t)(g.nx + 1); }

@@ -345,6 +345,14 @@ def sample_volume(volume, points, interp: str, stream=None):
     return out
 
 
+def sampler_peak(device: int = 0, kind: str = "layered") -> float:
+    """ctfp_sampler_peak: voxel-samples/s the texture path delivers at most
+    ('layered': two tld4 gathers per sample; 'tex3d': one filtered fetch)."""
+    r = C.c_double()
+    call("ctfp_sampler_peak", int(device), capi.SAMPLER_LAYERED if kind == "layered" else 0, C.byref(r))
+    return float(r.value)
+
+
 def build_grid_table(geometry: dict, grid, mu_strip, mu_inter, layout: int, device: int = 0):
     import torch
     g = make_geometry(geometry)

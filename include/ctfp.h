@@ -202,6 +202,15 @@ ctfp_status ctfp_backward(ctfp_plan* plan, const float* L_ckpt, const float* gI,
 ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float* const* g_volumes,
                                         void* stream);
 
+/* ---- sampler roofline --------------------------------------------------------
+ * No counterpart in the reference.  Measures, on `device`, the peak rate at
+ * which the texture path delivers trilinear footprints with nothing else to
+ * do: kind CTFP_SAMPLER_LAYERED times two 4-texel gathers (tld4) per
+ * voxel-sample, kind 0 one filtered tex3D fetch (the CTFP_INTERP_TEXTURE
+ * path), both from a texture that stays in the L1 texture cache, at full
+ * occupancy, with the march's warp shape.  Writes voxel-samples per second. */
+ctfp_status ctfp_sampler_peak(int32_t device, int32_t kind, double* voxel_samples_per_s);
+
 /* ---- launch-shape autotuner ------------------------------------------------
  * No counterpart in the reference (fixed 8 x 8 x 8 blocks,
  * Source/CUDAFun/CBCTPolyProjGPU.cuh:22-24).  Times candidate launch shapes of
@@ -224,10 +233,10 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * No counterpart in the reference, which simulates one phantom per process run
  * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
  * spectral tables; one device) and runs them with persistent kernels over a
- * device work queue: a work unit is one view x one 8 x 4 detector patch (the
- * 32 rays of one warp); items are grouped by material count and sampler mode
+ * device work queue: a work unit is one view x one 16 x 8 detector tile (the
+ * 128 rays of one CTA); items are grouped by material count and sampler mode
  * (one kernel per group, each with its own register budget) and queued
- * largest first (rays x samples x materials); every warp takes the next unit
+ * largest first (rays x samples x materials); every CTA takes the next unit
  * from an atomic counter.  A call is recorded once as a CUDA graph (volume
  * uploads, queue reset, kernels, fold) and replayed, in the order of the
  * stream passed, while the item pointers and the plans' tables stay the same;
