@@ -36,11 +36,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per full forward launch, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the 36-view case of the
-# same problem, scaled by views (traffic grows with the views marched); see
-# profiles/k_forward_layered_poly_grid_256.md.
-TRAFFIC_PER_LAUNCH = {}
+# DRAM bytes (read + write) per full forward launch, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of k_forward on the 36-view
+# case of the same problem (poly_grid_256_v36, default launch shape): 5.95 GB +
+# 0.09 GB, scaled by 10 for 360 views (traffic grows with the views marched).
+TRAFFIC_PER_LAUNCH = {("poly_grid_256", "trilinear"): 60.37e9}
 BYTES_PER_VOXEL_SAMPLE = 32  # 8 FP32 corners, the reuse-free trilinear footprint
 
 
@@ -213,6 +213,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--sampler", default="layered", choices=["layered", "global", "brick"],
+                    help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
                     help="problems in the uneven batch leg (0 skips it)")
     args = ap.parse_args()
@@ -249,6 +251,8 @@ def main():
     vols = physics.phantom(w, dev)
     M = len(vols)
     pr = Projector(w.geometry, M, args.interp, local)
+    if args.interp != "texture":
+        pr.set_sampler(args.sampler)
     pr.set_tables_from_workload(w)
     P, V, U = pr.shape_proj
     rays = P * U * V
@@ -288,16 +292,19 @@ def main():
     achieved = vs_launch * BYTES_PER_VOXEL_SAMPLE / (ms / 1e3) / 1e9
     vs_rate = vs_launch / (ms / 1e3)
     from ct_forward_projection_b200.projector import sampler_peak
-    tex_peak = sampler_peak(local, "tex3d" if args.interp == "texture" else "layered")
+    tex_peak = None
+    if args.interp == "texture" or args.sampler == "layered":
+        tex_peak = sampler_peak(local, "tex3d" if args.interp == "texture" else "layered")
     traffic = TRAFFIC_PER_LAUNCH.get((w.name, args.interp))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_rate,
                 "nominal_voxel_samples_per_launch": nominal_vs,
-                "texture": {"peak_voxel_samples_per_s": tex_peak, "achieved_voxel_samples_per_s": vs_rate,
-                            "frac": vs_rate / tex_peak, "binding": True,
-                            "peak_source": "ctfp_sampler_peak, measured in this run"},
-                "roof_min_hbm32_tex": min(peak * 1e9 / BYTES_PER_VOXEL_SAMPLE, tex_peak),
+                "texture": None if tex_peak is None else {
+                    "peak_voxel_samples_per_s": tex_peak, "achieved_voxel_samples_per_s": vs_rate,
+                    "frac": vs_rate / tex_peak, "binding": True,
+                    "peak_source": "ctfp_sampler_peak, measured in this run"},
+                "roof_min_hbm32_tex": None if tex_peak is None else min(peak * 1e9 / BYTES_PER_VOXEL_SAMPLE, tex_peak),
                 "note": ("achieved = 32 B (reuse-free 8-corner footprint) x support voxel-samples / kernel time; "
                          "the texture cache serves most corners, so DRAM traffic (ncu) is far below that and the "
                          "binding ceiling is the texture path (texture.frac)")}
@@ -363,7 +370,9 @@ def main():
             "value": value, "unit": "rays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded phantom per rank)",
-            "config": {"workload": w.name, "interp": args.interp, "volume": list(pr.shape_vol[::-1]), "materials": M,
+            "config": {"workload": w.name, "interp": args.interp,
+                       "sampler": args.sampler if args.interp != "texture" else "tex3d",
+                       "volume": list(pr.shape_vol[::-1]), "materials": M,
                        "views": P, "detector": [U, V], "energies": pr.E, "samples_per_ray": int(pr.info["intNum"]),
                        "rays_per_step": rays, "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": f"independent objects x{ws}"},
