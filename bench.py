@@ -14,8 +14,10 @@ per-pixel per-energy transmission.  A step is one full forward projection
             32 B (8 FP32 corners) per voxel-sample of algorithmic traffic
   cpu_baseline  the FP64 oracle on the host cores over a seeded ray subset
 
-Multi-GPU (torchrun): every rank projects its own seeded object (independent
-objects, weak scaling, no data-path collective); time is the max over ranks.
+Multi-GPU (torchrun): by default every rank projects its own seeded object
+(independent objects, weak scaling, no data-path collective); with --shard views
+the ranks split one object's views (strong scaling; the adjoint sums the ranks'
+partial gradients with an all-reduce).  Time is the max over ranks.
 --impl reference runs the reference's own implementation of the path (see
 reference_arm below).
 """
@@ -213,6 +215,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--shard", default="objects", choices=["objects", "views"],
+                    help="N > 1: each rank projects its own object (weak scaling) or a slab of one "
+                         "object's views (strong scaling; the adjoint sums gradients with all-reduce)")
     ap.add_argument("--sampler", default="layered", choices=["layered", "global", "brick"],
                     help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
@@ -227,7 +232,9 @@ def main():
 
     ws, rank, local = dist_setup(args.gpus)
     w = physics.workload(args.workload)
-    w.seed += rank  # each rank projects its own object
+    sharded = args.shard == "views" and ws > 1
+    if not sharded:
+        w.seed += rank  # each rank projects its own object
     dev = f"cuda:{local}"
 
     if args.impl == "reference":
@@ -256,7 +263,13 @@ def main():
     pr.set_tables_from_workload(w)
     P, V, U = pr.shape_proj
     rays = P * U * V
-    out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
+    vr = None  # this rank's (first view, count) when one object's views are sharded
+    if sharded:
+        from ct_forward_projection_b200.shard import view_range
+        vr = view_range(P, rank, ws)
+        args.batch_items = 0
+    n_local = vr[1] if sharded else P
+    out = {"I": torch.empty((n_local, V, U), device=dev), "IAbsorb": torch.empty((n_local, V, U), device=dev)}
     stream = torch.cuda.current_stream()
     shape = {"tile_u": 16, "tile_v": 8, "views_per_cta": 2, "min_ctas_per_sm": 4, "source": "default"}
     if not args.no_autotune:
@@ -267,7 +280,7 @@ def main():
 
     # ---------------- device-resident forward (value) -----------------------
     for _ in range(args.warmup):
-        pr.forward(vols, out=out)
+        pr.forward(vols, out=out, views=vr)
     barrier_sync(ws)
     clocks = ClockSampler(local)
     clocks.start()
@@ -276,17 +289,18 @@ def main():
     for s in range(args.steps):
         flush.fill_(float(s))
         ev[s][0].record(stream)
-        pr.forward(vols, out=out)
+        pr.forward(vols, out=out, views=vr)
         ev[s][1].record(stream)
     barrier_sync(ws)
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms = max_over_ranks(statistics.mean(step_ms), ws)
-    value = ws * rays / (ms / 1e3)
+    total_rays = rays if sharded else ws * rays
+    value = total_rays / (ms / 1e3)
 
     # roofline: algorithmic bytes of the dominant kernel per launch
     support = pr.count_support_samples()
-    vs_launch = support * M
+    vs_launch = support * M * n_local // P  # sharded: this rank's share of the views, pro rata
     nominal_vs = M * rays * int(pr.info["intNum"])
     peak, peak_kind = measured_peak_hbm()
     achieved = vs_launch * BYTES_PER_VOXEL_SAMPLE / (ms / 1e3) / 1e9
@@ -311,7 +325,7 @@ def main():
 
     # ---------------- end to end through ctfp_forward_host (e2e) ------------
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not sharded:
         host_vols = [v.cpu().pin_memory() for v in vols]
         host_out = {"I": torch.empty((P, V, U)).pin_memory(), "IAbsorb": torch.empty((P, V, U)).pin_memory(),
                     "I0": torch.empty((V, U)).pin_memory()}
@@ -336,18 +350,25 @@ def main():
     # forward with checkpoint, dLoss/dI in torch, the adjoint and the fold
     fa = None
     if not args.no_adjoint:
-        L = torch.empty((P, V, U, M), device=dev)
-        T = pr.forward([v * 0.97 for v in vols])["I"]
+        L = torch.empty((n_local, V, U, M), device=dev)
+        T = pr.forward([v * 0.97 for v in vols], views=vr)["I"]
         logT = torch.log(T)
         del T
         grads = [torch.zeros_like(v) for v in vols]
         loss = torch.zeros((), device=dev)
+        sp = None
+        if sharded:
+            from ct_forward_projection_b200.shard import ViewShardedProjector
+            sp = ViewShardedProjector(pr)
 
         def fa_step():
-            pr.forward(vols, out={**out, "L": L})
+            pr.forward(vols, out={**out, "L": L}, views=vr)
             r = torch.log(out["I"]) - logT
             loss.copy_(torch.sum(r * r))
-            pr.backward(L, 2.0 * r / out["I"], None, grads)
+            if sp is None:
+                pr.backward(L, 2.0 * r / out["I"], None, grads)
+            else:
+                sp.backward(L, gI=2.0 * r / out["I"], grads=grads)  # partial adjoint + all-reduce
 
         for _ in range(2):
             fa_step()
@@ -360,7 +381,7 @@ def main():
         e1.record(stream)
         barrier_sync(ws)
         fa_ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
-        fa = {"value": ws * rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms,
+        fa = {"value": total_rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms,
               "loss": "sum (log I - log T)^2, T = projection of the phantom x 0.97", "last_loss": float(loss)}
         del L, logT
 
@@ -381,14 +402,16 @@ def main():
         line = {
             "metric": "rays/s (polyenergetic cone-beam forward projection)",
             "value": value, "unit": "rays/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "strong" if sharded else "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded phantom per rank)",
             "config": {"workload": w.name, "interp": args.interp,
                        "sampler": args.sampler if args.interp != "texture" else "tex3d",
                        "volume": list(pr.shape_vol[::-1]), "materials": M,
                        "views": P, "detector": [U, V], "energies": pr.E, "samples_per_ray": int(pr.info["intNum"]),
                        "rays_per_step": rays, "l2": "flushed (256 MB write) between timed steps",
-                       "parallelism": f"independent objects x{ws}"},
+                       "parallelism": (f"one object, views sharded x{ws} (adjoint: all-reduce of gradients)"
+                                       if sharded else f"independent objects x{ws}")},
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -73,6 +73,8 @@ _SIGNATURES = {
     "ctfp_line_integrals": (C.c_int, [_P, _P, _P, _P]),
     "ctfp_forward": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "ctfp_spectral_from_L": (C.c_int, [_P, _P, _P, _P, _P]),
+    "ctfp_forward_views": (C.c_int, [_P, _P, C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
+    "ctfp_backward_views": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int64, _P, _P]),
     "ctfp_finalize_counts": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
     "ctfp_backward": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "ctfp_line_integrals_adjoint": (C.c_int, [_P, _P, _P, _P]),

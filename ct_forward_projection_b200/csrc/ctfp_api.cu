@@ -478,13 +478,17 @@ ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float
     return CTFP_OK;
 }
 
-ctfp_status ctfp_forward(ctfp_plan* p, const float* const* volumes, float* I, float* IAbsorb, float* I0,
-                         float* L_ckpt, void* stream)
+// The fused forward over views [view0, view0 + n_views); outputs hold those
+// views from index 0 when compact, else are full [projNum] arrays.
+static ctfp_status forward_range(ctfp_plan* p, const float* const* volumes, int64_t view0, int64_t n_views,
+                                 bool compact, float* I, float* IAbsorb, float* I0, float* L_ckpt, void* stream)
 {
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
     ctfp_status st = check_volumes(p, volumes);
     if (st != CTFP_OK) return st;
     if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    if (view0 < 0 || n_views < 0 || view0 + n_views > p->geom.projNum)
+        return fail(CTFP_INVALID_ARG, "view range outside [0, projNum)");
     DeviceScope ds(p->device);
     cudaStream_t s = (cudaStream_t)stream;
     MarchParams prm = base_params(p);
@@ -492,13 +496,28 @@ ctfp_status ctfp_forward(ctfp_plan* p, const float* const* volumes, float* I, fl
     prm.I = I;
     prm.IAbs = IAbsorb;
     prm.L = L_ckpt;
+    prm.view0 = (int)view0;
+    prm.n_views = (int)n_views;
+    prm.out_view0 = compact ? (int)view0 : 0;
     st = upload_textures(p, volumes, s);
     if (st != CTFP_OK) return st;
-    CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
+    if (n_views > 0) CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
     if (I0)
         CTFP_CUDA(cudaMemcpyAsync(I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
                                   cudaMemcpyDeviceToDevice, s));
     return CTFP_OK;
+}
+
+ctfp_status ctfp_forward(ctfp_plan* p, const float* const* volumes, float* I, float* IAbsorb, float* I0,
+                         float* L_ckpt, void* stream)
+{
+    return forward_range(p, volumes, 0, p ? p->geom.projNum : 0, false, I, IAbsorb, I0, L_ckpt, stream);
+}
+
+ctfp_status ctfp_forward_views(ctfp_plan* p, const float* const* volumes, int64_t view0, int64_t n_views, float* I,
+                               float* IAbsorb, float* I0, float* L_ckpt, void* stream)
+{
+    return forward_range(p, volumes, view0, n_views, true, I, IAbsorb, I0, L_ckpt, stream);
 }
 
 ctfp_status ctfp_forward_host(ctfp_plan* p, const float* const* host_volumes, float* host_I, float* host_IAbsorb,
@@ -555,12 +574,14 @@ ctfp_status ctfp_finalize_counts(int64_t n_pix, int64_t n_views, const float* I,
     return CTFP_OK;
 }
 
-ctfp_status ctfp_backward(ctfp_plan* p, const float* L_ckpt, const float* gI, const float* gIAbsorb,
-                          float* const* g_volumes, void* stream)
+static ctfp_status backward_range(ctfp_plan* p, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                                  int64_t view0, int64_t n_views, bool compact, float* const* g_volumes, void* stream)
 {
     if (!p || !L_ckpt || !g_volumes) return fail(CTFP_INVALID_ARG, "NULL argument");
     if (!gI && !gIAbsorb) return fail(CTFP_INVALID_ARG, "need gI or gIAbsorb");
     if (!p->spectral_ready) return fail(CTFP_NOT_READY, "spectral tables not set");
+    if (view0 < 0 || n_views < 0 || view0 + n_views > p->geom.projNum)
+        return fail(CTFP_INVALID_ARG, "view range outside [0, projNum)");
     for (int m = 0; m < p->M; m++)
         if (!g_volumes[m]) return fail(CTFP_INVALID_ARG, "gradient volume pointer is NULL");
     DeviceScope ds(p->device);
@@ -568,13 +589,29 @@ ctfp_status ctfp_backward(ctfp_plan* p, const float* L_ckpt, const float* gI, co
     prm.Lin = L_ckpt;
     prm.gI = gI;
     prm.gIAbs = gIAbsorb;
+    prm.view0 = (int)view0;
+    prm.n_views = (int)n_views;
+    prm.out_view0 = compact ? (int)view0 : 0;
     for (int m = 0; m < p->M; m++) prm.gvol[m] = g_volumes[m];
+    if (n_views == 0) return CTFP_OK;
     cudaStream_t s = (cudaStream_t)stream;
     ctfp_status st = prepare_expanded(p, prm, s);
     if (st != CTFP_OK) return st;
     CTFP_CUDA(launch_backward(prm, p->M, p->interp, false, p->shape, s));
     CTFP_CUDA(launch_fold(prm, p->M, s));
     return CTFP_OK;
+}
+
+ctfp_status ctfp_backward(ctfp_plan* p, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                          float* const* g_volumes, void* stream)
+{
+    return backward_range(p, L_ckpt, gI, gIAbsorb, 0, p ? p->geom.projNum : 0, false, g_volumes, stream);
+}
+
+ctfp_status ctfp_backward_views(ctfp_plan* p, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                                int64_t view0, int64_t n_views, float* const* g_volumes, void* stream)
+{
+    return backward_range(p, L_ckpt, gI, gIAbsorb, view0, n_views, true, g_volumes, stream);
 }
 
 ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* p, const float* gL, float* const* g_volumes, void* stream)

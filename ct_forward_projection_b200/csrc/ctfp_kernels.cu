@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256, MINB) k_forward(const MarchParams prm)
         if (p >= pend) break;
         float L[M];
         march_ray<M, MODE, SAMPLER>(prm, p, v, u, L);
-        const int64_t ray = (int64_t)p * npix + pix;
+        const int64_t ray = (int64_t)(p - prm.out_view0) * npix + pix;
         if (prm.L) store_L<M>(prm.L, ray, L);
         if (SPECTRAL) {
             float I, A;
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
     for (int k = 0; k < prm.views_per_cta; k++) {
         const int p = prm.view0 + blockIdx.y * prm.views_per_cta + k;
         if (p >= pend) break;
-        const int64_t ray = (int64_t)p * npix + pix;
+        const int64_t ray = (int64_t)(p - prm.out_view0) * npix + pix;
         float g[M];
         if (FROM_GL) {
             load_L<M>(prm.Lin, ray, g);
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kBU * kBV, MINB) k_forward_brick(const MarchPa
         float L[M];
 #pragma unroll
         for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
-        const int64_t ray = (int64_t)p * npix + pix;
+        const int64_t ray = (int64_t)(p - prm.out_view0) * npix + pix;
         if (prm.L) store_L<M>(prm.L, ray, L);
         if (SPECTRAL) {
             float I, A;

@@ -25,6 +25,7 @@ struct MarchParams {
     int view0;                        // first view of this launch
     int n_views;                      // views in this launch
     int views_per_cta;                // views each CTA marches for its pixel tile
+    int out_view0;                    // view stored at index 0 of I, IAbs, L, Lin, gI, gIAbs (0: full arrays)
 };
 
 struct LaunchShape {

@@ -174,18 +174,25 @@ class Projector:
             assert tuple(v.shape) == self.shape_vol, f"volume shape {tuple(v.shape)} != {self.shape_vol}"
         return ptr_array([_dptr(v) for v in volumes])
 
-    def forward(self, volumes: Sequence, want_L: bool = False, out=None, stream=None) -> dict:
-        """Fused march + spectral epilogue. Returns dict(I, IAbsorb, I0[, L])."""
+    def forward(self, volumes: Sequence, want_L: bool = False, out=None, stream=None, views=None) -> dict:
+        """Fused march + spectral epilogue. Returns dict(I, IAbsorb, I0[, L]).
+        views=(view0, n): only those views, in compact [n][V][U] outputs
+        (ctfp_forward_views)."""
         import torch
         dev = f"cuda:{self.device}"
         P, V, U = self.shape_proj
+        n = P if views is None else int(views[1])
         if out is None:
-            out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev),
+            out = {"I": torch.empty((n, V, U), device=dev), "IAbsorb": torch.empty((n, V, U), device=dev),
                    "I0": torch.empty((V, U), device=dev)}
             if want_L:
-                out["L"] = torch.empty((P, V, U, self.M), device=dev)
-        call("ctfp_forward", self._h, self._vol_ptrs(volumes), _dptr(out.get("I")), _dptr(out.get("IAbsorb")),
-             _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
+                out["L"] = torch.empty((n, V, U, self.M), device=dev)
+        if views is None:
+            call("ctfp_forward", self._h, self._vol_ptrs(volumes), _dptr(out.get("I")), _dptr(out.get("IAbsorb")),
+                 _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
+        else:
+            call("ctfp_forward_views", self._h, self._vol_ptrs(volumes), int(views[0]), n, _dptr(out.get("I")),
+                 _dptr(out.get("IAbsorb")), _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
         return out
 
     def forward_host(self, host_volumes: Sequence[np.ndarray], out: dict | None = None) -> dict:
@@ -215,13 +222,19 @@ class Projector:
         call("ctfp_spectral_from_L", self._h, _dptr(L), _dptr(out["I"]), _dptr(out["IAbsorb"]), _stream(stream))
         return out
 
-    def backward(self, L, gI=None, gIAbsorb=None, grads=None, stream=None) -> list:
-        """Adds dLoss/drho_m into grads (created as zeros if None)."""
+    def backward(self, L, gI=None, gIAbsorb=None, grads=None, stream=None, views=None) -> list:
+        """Adds dLoss/drho_m into grads (created as zeros if None).
+        views=(view0, n): L, gI, gIAbsorb are the compact buffers of those
+        views (ctfp_backward_views)."""
         import torch
         if grads is None:
             grads = [torch.zeros(self.shape_vol, device=f"cuda:{self.device}") for _ in range(self.M)]
-        call("ctfp_backward", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), ptr_array([_dptr(g) for g in grads]),
-             _stream(stream))
+        gp = ptr_array([_dptr(g) for g in grads])
+        if views is None:
+            call("ctfp_backward", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), gp, _stream(stream))
+        else:
+            call("ctfp_backward_views", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), int(views[0]), int(views[1]),
+                 gp, _stream(stream))
         return grads
 
     def line_integrals_adjoint(self, gL, grads=None, stream=None) -> list:

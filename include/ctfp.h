@@ -271,6 +271,18 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* co
 ctfp_status ctfp_batch_info(const ctfp_batch* batch, int64_t* total_units, int32_t* grid_forward,
                             int32_t* grid_adjoint);
 
+/* ---- view ranges (sharding one object's views across GPUs) -----------------
+ * No counterpart in the reference.  The forward and the adjoint over views
+ * [view0, view0 + n_views) only, with compact buffers: I, IAbsorb, L_ckpt,
+ * gI and gIAbsorb hold those views from index 0 ([n_views][dNumV][dNumU],
+ * L_ckpt [n_views][dNumV][dNumU][M]).  Each GPU of a view-sharded projection
+ * runs its own range on its own plan; the gradient volumes are partial sums
+ * over the range (sum them across GPUs).  n_views = 0 is a no-op. */
+ctfp_status ctfp_forward_views(ctfp_plan* plan, const float* const* volumes, int64_t view0, int64_t n_views,
+                               float* I, float* IAbsorb, float* I0, float* L_ckpt, void* stream);
+ctfp_status ctfp_backward_views(ctfp_plan* plan, const float* L_ckpt, const float* gI, const float* gIAbsorb,
+                                int64_t view0, int64_t n_views, float* const* g_volumes, void* stream);
+
 /* ---- forward without device allocation -------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code running inside a host framework that owns all device memory through its
