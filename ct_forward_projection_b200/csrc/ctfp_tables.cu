@@ -45,31 +45,48 @@ __device__ __forceinline__ float unit_height(const GridUnits& gu, long long j, f
     return gu.h / gu.FD * sqrtf(gu.FD * gu.FD + dc * dc + y * y);
 }
 
-// Transmission of 1-um unit i: the closed form of the fill loops of
-// createDiscreteGrid_u{E,O}d{E,O} (Grid.cpp:90-270) followed by their mirror.
-__device__ float unit_transmission(const GridUnits& gu, long long i, float y)
+// Sum of the 1-um unit transmissions over the mirrored-index range
+// [jlo, jhi]: the closed form of the fill loops of createDiscreteGrid_u{E,O}d{E,O}
+// (Grid.cpp:90-270).  Units j > start form the central interspace half-gap,
+// each with its own height (Grid.cpp:93-96, 137-141, 181-184, 226-230); below
+// it the pattern repeats with period sw + iw counted leftwards from start:
+// strip units with their own heights (Grid.cpp:107), interspace units with the
+// height of their period's first unit (Grid.cpp:115).  Interspace units of one
+// period therefore share one transmission, and each run of them contributes its
+// length times that value.
+__device__ double sum_units(const GridUnits& gu, long long jlo, long long jhi, float y)
 {
-    long long j = i;
-    const long long c = gu.c;
-    // mirror the right half onto the left half
-    if (!gu.uOdd && !gu.iOdd) {
-        if (i >= c) j = gu.N - i - 1;          // Grid.cpp:126-129
-    } else if (!gu.uOdd && gu.iOdd) {
-        if (i >= c + 1) j = gu.N - i;          // Grid.cpp:170-173
-    } else if (gu.uOdd && !gu.iOdd) {
-        if (i >= c + 1) j = gu.N - i;          // Grid.cpp:214-217
-    } else {
-        if (i >= c + 1) j = gu.N - i - 1;      // Grid.cpp:260-263
+    double sum = 0.0;
+    long long j = jhi;
+    // central half-gap (j > start), own unit heights
+    for (; j >= jlo && j > gu.start; j--) sum += (double)expf(-gu.mi * unit_height(gu, j, y));
+    while (j >= jlo) {
+        const long long k = gu.start - j;
+        const long long q = k / gu.period, r = k % gu.period;
+        if (r < gu.sw) {
+            // strip units of this period, down to the strip's end or jlo
+            const long long jend = max(jlo, j - (gu.sw - 1 - r));
+            for (; j >= jend; j--) sum += (double)expf(-gu.ms * unit_height(gu, j, y));
+        } else {
+            // interspace units of this period share one transmission
+            const long long jend = max(jlo, j - (gu.period - 1 - r));
+            const float t = expf(-gu.mi * unit_height(gu, gu.start - q * gu.period, y));
+            sum += (double)t * (double)(j - jend + 1);
+            j = jend - 1;
+        }
     }
-    if (j > gu.start) {
-        // central interspace half-gap, own unit height (Grid.cpp:93-96, 137-141, 181-184, 226-230)
-        return expf(-gu.mi * unit_height(gu, j, y));
-    }
-    const long long k = gu.start - j;
-    const long long q = k / gu.period, r = k % gu.period;
-    if (r < gu.sw) return expf(-gu.ms * unit_height(gu, j, y));  // strip (Grid.cpp:107)
-    // interspace: height of the period-start unit (Grid.cpp:115)
-    return expf(-gu.mi * unit_height(gu, gu.start - q * gu.period, y));
+    return sum;
+}
+
+// First unit of the mirrored (right) half and the mirror image of a unit
+// there, per parity case (Grid.cpp:126-129, 170-173, 214-217, 260-263).
+__device__ __forceinline__ long long mirror_start(const GridUnits& gu)
+{
+    return (!gu.uOdd && !gu.iOdd) ? gu.c : gu.c + 1;
+}
+__device__ __forceinline__ long long mirror_of(const GridUnits& gu, long long i)
+{
+    return ((!gu.uOdd && !gu.iOdd) || (gu.uOdd && gu.iOdd)) ? gu.N - i - 1 : gu.N - i;
 }
 
 __global__ void k_grid(GridUnits gu, int E, const float* __restrict__ mus, const float* __restrict__ mui, int U,
@@ -87,9 +104,14 @@ __global__ void k_grid(GridUnits gu, int E, const float* __restrict__ mus, const
         g.mi = mui[e] / 1000.0f;  // (Grid.cpp:411)
         float y = 0.f;
         if (layout == CTFP_GRID_PIXEL) y = dHalfLV_um - dSize_um / 2 - (float)v * dSize_um;
-        double sum = 0.0;  // binning1D accumulates in double (Grid.cpp:299-306)
-        const long long i0 = (long long)u * gu.dSize;
-        for (int k = 0; k < gu.dSize; k++) sum += (double)unit_transmission(g, i0 + k, y);
+        // binning1D: mean over the pixel's units, accumulated in double
+        // (Grid.cpp:299-306); units left of the mirror map to themselves,
+        // units right of it to their mirror images
+        const long long i0 = (long long)u * gu.dSize, i1 = i0 + gu.dSize - 1;
+        const long long m = mirror_start(g);
+        double sum = 0.0;
+        if (i0 < m) sum += sum_units(g, i0, min(i1, m - 1), y);
+        if (i1 >= m) sum += sum_units(g, mirror_of(g, i1), mirror_of(g, max(i0, m)), y);
         out[t] = (float)(sum / (double)gu.dSize);
     }
 }
