@@ -41,6 +41,10 @@ struct ctfp_plan {
     cudaTextureObject_t ltex[kMaxM] = {};
     LaunchShape shape{};
     unsigned long long* d_count = nullptr;
+    // empty-space skipping (off by default): brick occupancy, rebuilt from the
+    // volumes at every call
+    bool skip_empty = false;
+    uint8_t* d_occ = nullptr;
     // corner-expanded adjoint accumulators (allocated on first backward)
     float4* d_gexp[kMaxM] = {};
     // staging for ctfp_forward_host
@@ -246,7 +250,23 @@ MarchParams base_params(const ctfp_plan* p)
         prm.tex[m] = p->tex[m];
         prm.ltex[m] = p->ltex[m];
     }
+    if (p->skip_empty && p->d_occ) {
+        prm.occ = p->d_occ;
+        prm.occ_x = occ_dim(p->gp.nx);
+        prm.occ_y = occ_dim(p->gp.ny);
+    }
     return prm;
+}
+
+// Sampler copies of the caller's volumes and, with empty-space skipping, the
+// brick occupancy, on stream st.
+ctfp_status prepare_volumes(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
+{
+    ctfp_status rs = upload_textures(p, volumes, st);
+    if (rs != CTFP_OK) return rs;
+    if (p->skip_empty && p->d_occ)
+        CTFP_CUDA(launch_occupancy(volumes, p->M, p->gp.nx, p->gp.ny, p->gp.nz, p->d_occ, st));
+    return CTFP_OK;
 }
 
 // Zeroed corner-expanded accumulators for one adjoint launch.
@@ -381,6 +401,7 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     cudaFree(p->d_count);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->d_gexp[m]);
+    cudaFree(p->d_occ);
     cudaFree(p->d2h_I);
     cudaFree(p->d2h_IAbs);
     delete p;
@@ -472,7 +493,7 @@ ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float
     MarchParams prm = base_params(p);
     for (int m = 0; m < p->M; m++) prm.vol[m] = volumes[m];
     prm.L = L;
-    st = upload_textures(p, volumes, s);
+    st = prepare_volumes(p, volumes, s);
     if (st != CTFP_OK) return st;
     CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, false, p->shape, s));
     return CTFP_OK;
@@ -499,7 +520,7 @@ static ctfp_status forward_range(ctfp_plan* p, const float* const* volumes, int6
     prm.view0 = (int)view0;
     prm.n_views = (int)n_views;
     prm.out_view0 = compact ? (int)view0 : 0;
-    st = upload_textures(p, volumes, s);
+    st = prepare_volumes(p, volumes, s);
     if (st != CTFP_OK) return st;
     if (n_views > 0) CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
     if (I0)
@@ -712,9 +733,22 @@ ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t 
 {
     ctfp_status s = check_volumes(p, volumes);
     if (s != CTFP_OK) return s;
-    return upload_textures(p, volumes, st);
+    return prepare_volumes(p, volumes, st);
 }
 }  // namespace ctfp
+
+extern "C" ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* p, int32_t enable)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    DeviceScope ds(p->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    if (enable && !p->d_occ) {
+        const size_t n = (size_t)occ_dim(p->gp.nx) * occ_dim(p->gp.ny) * occ_dim(p->gp.nz);
+        CTFP_CUDA(cudaMalloc(&p->d_occ, n));
+    }
+    p->skip_empty = enable != 0;
+    return CTFP_OK;
+}
 
 extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,
                                                   int32_t min_ctas_per_sm)

@@ -19,6 +19,8 @@ namespace ctfp {
 enum { INTERP_TRILINEAR = 0, INTERP_TEXEMU = 1, INTERP_TEXTURE = 2 };
 // Where the software samplers (TRILINEAR, TEXEMU) read their 8 corners.
 enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2, SAMPLER_BRICK = 3 };
+// Kernel-internal: the layered sampler with empty-space skipping.
+enum { SAMPLER_LAYERED_SKIP = 4 };
 constexpr int kMaxM = 4;
 
 // Scalar geometry shared by every ray of one problem.

@@ -20,15 +20,27 @@ namespace {
 template <int M, int SAMPLER>
 __device__ __forceinline__ void load_corners(const MarchParams& prm, const Corner& c, float (*v)[8])
 {
-    if (SAMPLER == SAMPLER_LAYERED) load8_layered<M>(prm.ltex, prm.g.nz, c, v);
+    if (SAMPLER == SAMPLER_LAYERED || SAMPLER == SAMPLER_LAYERED_SKIP) load8_layered<M>(prm.ltex, prm.g.nz, c, v);
     else load8_global<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, v);
 }
 
+// Whether the footprint with base corner c can read a non-zero voxel (brick
+// occupancy); bases outside [-1, n - 1] read only the border.
+__device__ __forceinline__ bool footprint_occupied(const MarchParams& prm, const Corner& c)
+{
+    const unsigned x = (unsigned)(c.ix + 1), y = (unsigned)(c.iy + 1), z = (unsigned)(c.iz + 1);
+    if (x > (unsigned)prm.g.nx || y > (unsigned)prm.g.ny || z > (unsigned)prm.g.nz) return false;
+    const size_t b = ((size_t)(z >> kOccShift) * prm.occ_y + (y >> kOccShift)) * prm.occ_x + (x >> kOccShift);
+    return __ldg(prm.occ + b) != 0;
+}
+
 // One sample of a software-interpolated march: fetch the footprint,
-// interpolate, accumulate.
+// interpolate, accumulate.  With empty-space skipping, a footprint inside an
+// all-zero brick contributes exactly zero and is not fetched.
 template <int M, int MODE, int SAMPLER>
 __device__ __forceinline__ void sample_acc(const MarchParams& prm, const Corner& c, float* acc, float* cmp)
 {
+    if (SAMPLER == SAMPLER_LAYERED_SKIP && !footprint_occupied(prm, c)) return;
     float v[M][8];
     load_corners<M, SAMPLER>(prm, c, v);
 #pragma unroll
@@ -547,9 +559,13 @@ cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, b
     const bool lay = sampler == SAMPLER_LAYERED;
     switch (interp) {
         case INTERP_TRILINEAR:
+            if (lay && prm.occ)
+                return fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_LAYERED_SKIP>(prm, spec, minb, grid, block, smem, st);
             return lay ? fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_LAYERED>(prm, spec, minb, grid, block, smem, st)
                        : fwd_dispatch_spec<M, INTERP_TRILINEAR, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
         case INTERP_TEXEMU:
+            if (lay && prm.occ)
+                return fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED_SKIP>(prm, spec, minb, grid, block, smem, st);
             return lay ? fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED>(prm, spec, minb, grid, block, smem, st)
                        : fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
         case INTERP_TEXTURE:
@@ -704,6 +720,50 @@ cudaError_t launch_sample_points(const float* vol, cudaTextureObject_t tex, int 
     if (nb > 148 * 32) nb = 148 * 32;
     if (nb == 0) return cudaSuccess;
     k_sample_points<<<(unsigned)nb, 256, 0, st>>>(vol, tex, nx, ny, nz, interp, pts, n, out);
+    return cudaGetLastError();
+}
+
+namespace {
+
+// One thread per voxel: a non-zero voxel marks every brick whose dilated
+// range [8b - 1, 8b + 7] holds it (b = (x + 1) >> 3, and b - 1 when x + 1 is a
+// multiple of 8), per axis.  Concurrent stores all write 1.
+struct VolPtrs {
+    const float* p[kMaxM];
+};
+
+__global__ void k_occupancy(const VolPtrs vol, int M, int nx, int ny, int nz, int ox, int oy, uint8_t* occ)
+{
+    const int64_t n = (int64_t)nx * ny * nz;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        bool any = false;
+        for (int m = 0; m < M; m++) any |= __ldg(vol.p[m] + k) != 0.f;
+        if (!any) continue;
+        const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((int64_t)nx * ny));
+        const int bx = (x + 1) >> kOccShift, by = (y + 1) >> kOccShift, bz = (z + 1) >> kOccShift;
+        const int lx = ((x + 1) & ((1 << kOccShift) - 1)) == 0 && bx > 0;
+        const int ly = ((y + 1) & ((1 << kOccShift) - 1)) == 0 && by > 0;
+        const int lz = ((z + 1) & ((1 << kOccShift) - 1)) == 0 && bz > 0;
+        for (int dz = 0; dz <= lz; dz++)
+            for (int dy = 0; dy <= ly; dy++)
+                for (int dx = 0; dx <= lx; dx++)
+                    occ[((size_t)(bz - dz) * oy + (by - dy)) * ox + (bx - dx)] = 1;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st)
+{
+    const int ox = occ_dim(nx), oy = occ_dim(ny), oz = occ_dim(nz);
+    cudaError_t e = cudaMemsetAsync(occ, 0, (size_t)ox * oy * oz, st);
+    if (e != cudaSuccess) return e;
+    VolPtrs vp = {};
+    for (int m = 0; m < M && m < kMaxM; m++) vp.p[m] = vol[m];
+    const int64_t n = (int64_t)nx * ny * nz;
+    int64_t nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    k_occupancy<<<(unsigned)nb, 256, 0, st>>>(vp, M, nx, ny, nz, ox, oy, occ);
     return cudaGetLastError();
 }
 

@@ -26,7 +26,16 @@ struct MarchParams {
     int n_views;                      // views in this launch
     int views_per_cta;                // views each CTA marches for its pixel tile
     int out_view0;                    // view stored at index 0 of I, IAbs, L, Lin, gI, gIAbs (0: full arrays)
+    const uint8_t* occ;               // empty-space skipping: brick occupancy (null: march every sample)
+    int occ_x, occ_y;                 // bricks along x, y (see launch_occupancy)
 };
+
+// Bricks of kOccShift^2 voxels per axis for empty-space skipping.  Brick
+// (bx, by, bz) is marked when any material has a non-zero voxel in
+// [8b - 1, 8b + 7] on every axis: exactly the voxels a footprint with base
+// corner ix in [8b - 1, 8b + 6] (brick of ix + 1) can read.
+constexpr int kOccShift = 3;
+inline int occ_dim(int n) { return ((n + 1) >> kOccShift) + 1; }
 
 struct LaunchShape {
     int tile_u = 16, tile_v = 8, views_per_cta = 2;
@@ -52,5 +61,8 @@ cudaError_t launch_finalize(int64_t n_pix, int64_t n_views, const float* I, cons
 cudaError_t launch_sample_points(const float* vol, cudaTextureObject_t tex, int nx, int ny, int nz, int interp,
                                  const float* pts, int64_t n, float* out, cudaStream_t st);
 cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, cudaStream_t st);
+// Fills occ [occ_dim(nz)][occ_dim(ny)][occ_dim(nx)] from the M volumes
+// (vol: host array of M device pointers; occ is zeroed first).
+cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st);
 
 }  // namespace ctfp

@@ -118,6 +118,10 @@ class Projector:
         call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED,
                                                  "brick": capi.SAMPLER_BRICK}[sampler])
 
+    def set_skip_empty(self, enable: bool = True) -> None:
+        """Empty-space skipping for the layered sampler (ctfp_plan_set_skip_empty)."""
+        call("ctfp_plan_set_skip_empty", self._h, 1 if enable else 0)
+
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)
 

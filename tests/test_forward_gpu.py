@@ -241,3 +241,53 @@ def test_brick_sampler_equals_layered(cuda_ok, mode, pitch):
         b = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
     assert torch.equal(a["L"], b["L"]) and torch.equal(a["I"], b["I"]) and torch.equal(a["IAbsorb"], b["IAbsorb"])
+
+
+def _sparse_volumes(d, M, seed):
+    # random densities with large all-zero regions (as air around a body)
+    vols = random_volumes(d, M, seed)
+    z, y, x = vols[0].shape
+    for v in vols:
+        v[:, :, : x // 3] = 0.0
+        v[: z // 2, y // 2:, :] = 0.0
+    return vols
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("M", [1, 2, 3])
+def test_skip_empty_matches_full_march(cuda_ok, mode, M):
+    d = small_geometry(n=(40, 36, 30), views=6, U=37, V=29)
+    vols = _sparse_volumes(d, M, 40 + M)
+    S, mu, G, D = spectral_setup(d, M, 7, 3)
+    with Projector(d, M, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        full = pr.forward(to_dev(vols), want_L=True)
+        pr.set_skip_empty(True)
+        skip = pr.forward(to_dev(vols), want_L=True)
+        skip2 = pr.forward(to_dev(vols), want_L=True)  # occupancy rebuilt per call
+        torch.cuda.synchronize()
+    for k in ("I", "IAbsorb"):
+        assert rel_err(skip[k].cpu().numpy(), full[k].cpu().numpy()) < 1e-6
+    assert rel_err_scaled(skip["L"].cpu().numpy(), full["L"].cpu().numpy()) < 1e-6
+    assert torch.equal(skip["I"], skip2["I"])
+    if mode == "trilinear":
+        W = O.energy_weights(d, S, G, 2, D, 1000.0)
+        ref = O.forward(d, vols, mu, W, O.TRILINEAR)
+        assert rel_err(skip["I"].cpu().numpy(), ref["I"]) < RTOL_TRI
+
+
+@pytest.mark.parametrize("pos", [(0, 0, 0), (6, 7, 8), (7, 15, 23), (8, 16, 24), (15, 9, 31), (31, 31, 31)])
+def test_skip_empty_isolated_voxels_at_brick_edges(cuda_ok, pos):
+    # one non-zero voxel on either side of the 8-voxel brick boundaries and at
+    # the volume's faces: a brick missed by the dilation would drop every ray
+    # through that voxel's footprint
+    d = small_geometry(n=32, views=5, U=41, V=41, pitch=0.9)
+    vol = np.zeros((32, 32, 32), np.float32)
+    vol[pos[2], pos[1], pos[0]] = 1.5
+    with Projector(d, 1, "trilinear") as pr:
+        full = pr.line_integrals(to_dev([vol])).cpu().numpy()
+        pr.set_skip_empty(True)
+        skip = pr.line_integrals(to_dev([vol])).cpu().numpy()
+    assert np.count_nonzero(full) > 0
+    np.testing.assert_array_equal(skip != 0, full != 0)
+    assert rel_err_scaled(skip, full) < 1e-6
