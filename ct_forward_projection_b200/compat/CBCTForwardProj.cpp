@@ -71,14 +71,6 @@ std::vector<float> read_table(const std::string& path, int n, const char* what)
 }
 
 // MSVC CRT rand() (the reference was built with it): state * 214013 + 2531011.
-struct MsvcRand {
-    unsigned int state = 1u;
-    int next()
-    {
-        state = state * 214013u + 2531011u;
-        return (int)((state >> 16) & 0x7fffu);
-    }
-};
 
 }  // namespace
 
@@ -178,28 +170,13 @@ void CBCTForwardProj::updateDetResponse()
             (1 - expf(-h_mForwardProj.scintillatorLineAtten[specIndex] * h_mForwardProj.scintillatorPerThickness[i]));
 }
 
-// Per-view focal-spot offsets (CBCTForwardProj.cpp:122-148).  The blur path
-// that consumes them is unreachable in the reference and not rebuilt.
+// Per-view focal-spot offsets (CBCTForwardProj.cpp:122-148), mm.
 void CBCTForwardProj::computeFoSpOffset()
 {
     if (!h_mForwardProj.foSpOffsetU) h_mForwardProj.foSpOffsetU = new float[mCTScanParas.projNum];
     if (!h_mForwardProj.foSpOffsetV) h_mForwardProj.foSpOffsetV = new float[mCTScanParas.projNum];
-    MsvcRand r;
-    r.state = 10u;
-    const float radius = mCTScanParas.focalSpotSize / 2.0f;
-    const int size = (int)(mCTScanParas.focalSpotSize * 10000);
-    const float pi = acosf(-1.0f);
-    for (size_t i = 0; i < mCTScanParas.projNum; i++) {
-        float du = 0.f, dv = 0.f;
-        if (size > 0) {
-            do {
-                du = -radius + (r.next() % size) / 10000.0f;
-                dv = -radius + (r.next() % size) / 10000.0f;
-            } while (du * du + dv * dv > pi * radius * radius);
-        }
-        h_mForwardProj.foSpOffsetU[i] = du;
-        h_mForwardProj.foSpOffsetV[i] = dv;
-    }
+    CTFP_CHECK(ctfp_focal_spot_offsets((int64_t)mCTScanParas.projNum, mCTScanParas.focalSpotSize,
+                                       h_mForwardProj.foSpOffsetU, h_mForwardProj.foSpOffsetV));
 }
 
 // Normalised spectrum, SpecEnergyNum values (CBCTForwardProj.cpp:150-171).
@@ -325,6 +302,8 @@ void CBCTForwardProj::runDeviceProjection(bool grid, bool response, bool single)
 
     PlanGuard plan;
     CTFP_CHECK(ctfp_plan_create(&g, M, interp_from_env(), 0, &plan.p));
+    if (focalSpot_)
+        CTFP_CHECK(ctfp_plan_set_focal_spot(plan.p, h_mForwardProj.foSpOffsetU, h_mForwardProj.foSpOffsetV));
     DeviceBuffers db;
 
     // density maps: label -> rho_m (multi-material), label * density[0] (single)

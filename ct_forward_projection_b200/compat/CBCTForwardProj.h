@@ -104,6 +104,7 @@ protected:
     size_t nPix() const { return mCTScanParas.dNumU * mCTScanParas.dNumV; }
     void freeResults();
 
+    bool focalSpot_ = false;         // runDeviceProjection applies h_mForwardProj.foSpOffset{U,V}
     std::vector<float> gridTable_;   // [E][U] grid transmission
     std::vector<float> detTable_;    // [E][V][U] detector response
 };

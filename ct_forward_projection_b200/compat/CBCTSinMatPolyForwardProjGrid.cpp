@@ -23,7 +23,20 @@ void CBCTSinMatPolyForwardProjGrid::computePolyForwProjNoResponse()
     saveAll(false);
 }
 
+// CBCTSinMatPolyForwardProjGrid.cpp:269-388: the same outputs as
+// computePolyForwProj, with per-view focal-spot offsets (computeFoSpOffset)
+// shifting each view's sampling and re-aligning its projection.
 void CBCTSinMatPolyForwardProjGrid::computePolyForwProjFoSp()
 {
-    throw std::runtime_error("the focal-spot path is unreachable in the reference and not rebuilt");
+    std::cout << "single-material forward projection with grid, focal spot ====>>>>" << std::endl;
+    computeFoSpOffset();
+    focalSpot_ = true;
+    try {
+        runDeviceProjection(true, true, true);
+    } catch (...) {
+        focalSpot_ = false;
+        throw;
+    }
+    focalSpot_ = false;
+    saveAll(true);
 }

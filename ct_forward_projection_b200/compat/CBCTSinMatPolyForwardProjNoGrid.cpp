@@ -22,7 +22,20 @@ void CBCTSinMatPolyForwardProjNoGrid::computePolyForwProjNoResponse()
     saveAll(false);
 }
 
+// CBCTSinMatPolyForwardProjNoGrid.cpp:216-331: the same outputs as
+// computePolyForwProj, with per-view focal-spot offsets (computeFoSpOffset)
+// shifting each view's sampling and re-aligning its projection.
 void CBCTSinMatPolyForwardProjNoGrid::computePolyForwProjFoSp()
 {
-    throw std::runtime_error("the focal-spot path is unreachable in the reference and not rebuilt");
+    std::cout << "single-material forward projection without grid, focal spot ====>>>>" << std::endl;
+    computeFoSpOffset();
+    focalSpot_ = true;
+    try {
+        runDeviceProjection(false, true, true);
+    } catch (...) {
+        focalSpot_ = false;
+        throw;
+    }
+    focalSpot_ = false;
+    saveAll(true);
 }

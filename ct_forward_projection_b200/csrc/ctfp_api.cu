@@ -45,6 +45,13 @@ struct ctfp_plan {
     // volumes at every call
     bool skip_empty = false;
     uint8_t* d_occ = nullptr;
+    // focal spot (off unless set): per-view offsets, and the march's raw
+    // line integrals before the re-alignment (grown on demand)
+    float2* d_fspot = nullptr;
+    float* d_fs_raw = nullptr;
+    size_t fs_raw_elems = 0;
+    float* d_fs_L = nullptr;
+    size_t fs_L_elems = 0;
     // corner-expanded adjoint accumulators (allocated on first backward)
     float4* d_gexp[kMaxM] = {};
     // staging for ctfp_forward_host
@@ -258,6 +265,37 @@ MarchParams base_params(const ctfp_plan* p)
     return prm;
 }
 
+// Device scratch of at least n floats, grown on demand.
+ctfp_status ensure_scratch(float*& ptr, size_t& have, size_t n)
+{
+    if (n <= have) return CTFP_OK;
+    cudaFree(ptr);
+    ptr = nullptr;
+    have = 0;
+    CTFP_CUDA(cudaMalloc(&ptr, n * sizeof(float)));
+    have = n;
+    return CTFP_OK;
+}
+
+// The march over views [view0, view0 + n) with a focal spot: raw line
+// integrals into plan scratch, then the re-alignment into L (compact).
+ctfp_status focal_spot_march(ctfp_plan* p, MarchParams prm, int64_t view0, int64_t n, float* L, cudaStream_t s)
+{
+    const size_t elems = (size_t)n * p->geom.dNumU * p->geom.dNumV * p->M;
+    ctfp_status st = ensure_scratch(p->d_fs_raw, p->fs_raw_elems, elems);
+    if (st != CTFP_OK) return st;
+    prm.view0 = (int)view0;
+    prm.n_views = (int)n;
+    prm.out_view0 = (int)view0;
+    prm.L = p->d_fs_raw;
+    prm.I = nullptr;
+    prm.IAbs = nullptr;
+    prm.occ = nullptr;  // the image shift reads neighbouring rays: march them all
+    CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, false, p->shape, s));
+    CTFP_CUDA(launch_shift_views(p->d_fs_raw, L, p->gp, p->M, p->interp, (int)view0, (int)n, s));
+    return CTFP_OK;
+}
+
 // Sampler copies of the caller's volumes and, with empty-space skipping, the
 // brick occupancy, on stream st.
 ctfp_status prepare_volumes(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
@@ -402,6 +440,9 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->d_gexp[m]);
     cudaFree(p->d_occ);
+    cudaFree(p->d_fspot);
+    cudaFree(p->d_fs_raw);
+    cudaFree(p->d_fs_L);
     cudaFree(p->d2h_I);
     cudaFree(p->d2h_IAbs);
     delete p;
@@ -495,6 +536,7 @@ ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float
     prm.L = L;
     st = prepare_volumes(p, volumes, s);
     if (st != CTFP_OK) return st;
+    if (p->gp.fspot) return focal_spot_march(p, prm, 0, p->geom.projNum, L, s);
     CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, false, p->shape, s));
     return CTFP_OK;
 }
@@ -522,7 +564,28 @@ static ctfp_status forward_range(ctfp_plan* p, const float* const* volumes, int6
     prm.out_view0 = compact ? (int)view0 : 0;
     st = prepare_volumes(p, volumes, s);
     if (st != CTFP_OK) return st;
-    if (n_views > 0) CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
+    if (n_views > 0 && p->gp.fspot) {
+        // focal spot: march, re-align the line-integral images, then the
+        // spectral epilogue on the re-aligned integrals
+        const int64_t npix = p->geom.dNumU * p->geom.dNumV;
+        const int64_t skip = compact ? 0 : view0;
+        float* Ldst = L_ckpt ? L_ckpt + skip * npix * p->M : nullptr;
+        if (!Ldst) {
+            st = ensure_scratch(p->d_fs_L, p->fs_L_elems, (size_t)n_views * npix * p->M);
+            if (st != CTFP_OK) return st;
+            Ldst = p->d_fs_L;
+        }
+        st = focal_spot_march(p, prm, view0, n_views, Ldst, s);
+        if (st != CTFP_OK) return st;
+        MarchParams sp = base_params(p);
+        sp.g.P = (int)n_views;
+        sp.Lin = Ldst;
+        sp.I = I ? I + skip * npix : nullptr;
+        sp.IAbs = IAbsorb ? IAbsorb + skip * npix : nullptr;
+        CTFP_CUDA(launch_spectral_from_L(sp, p->M, s));
+    } else if (n_views > 0) {
+        CTFP_CUDA(launch_forward(prm, p->M, p->interp, p->sampler, true, p->shape, s));
+    }
     if (I0)
         CTFP_CUDA(cudaMemcpyAsync(I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
                                   cudaMemcpyDeviceToDevice, s));
@@ -605,6 +668,7 @@ static ctfp_status backward_range(ctfp_plan* p, const float* L_ckpt, const float
         return fail(CTFP_INVALID_ARG, "view range outside [0, projNum)");
     for (int m = 0; m < p->M; m++)
         if (!g_volumes[m]) return fail(CTFP_INVALID_ARG, "gradient volume pointer is NULL");
+    if (p->gp.fspot) return fail(CTFP_UNSUPPORTED, "the adjoint does not model a focal spot");
     DeviceScope ds(p->device);
     MarchParams prm = base_params(p);
     prm.Lin = L_ckpt;
@@ -640,6 +704,7 @@ ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* p, const float* gL, float* co
     if (!p || !gL || !g_volumes) return fail(CTFP_INVALID_ARG, "NULL argument");
     for (int m = 0; m < p->M; m++)
         if (!g_volumes[m]) return fail(CTFP_INVALID_ARG, "gradient volume pointer is NULL");
+    if (p->gp.fspot) return fail(CTFP_UNSUPPORTED, "the adjoint does not model a focal spot");
     DeviceScope ds(p->device);
     MarchParams prm = base_params(p);
     prm.Lin = gL;
@@ -736,6 +801,61 @@ ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t 
     return prepare_volumes(p, volumes, st);
 }
 }  // namespace ctfp
+
+extern "C" ctfp_status ctfp_plan_set_focal_spot(ctfp_plan* p, const float* offset_u, const float* offset_v)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    if (!offset_u != !offset_v) return fail(CTFP_INVALID_ARG, "give both offset arrays or neither");
+    DeviceScope ds(p->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    if (!offset_u) {
+        p->gp.fspot = nullptr;
+        return CTFP_OK;
+    }
+    const size_t P = (size_t)p->geom.projNum;
+    std::vector<float2> f(P);
+    for (size_t k = 0; k < P; k++) {
+        if (!std::isfinite(offset_u[k]) || !std::isfinite(offset_v[k]))
+            return fail(CTFP_INVALID_ARG, "focal-spot offsets must be finite");
+        f[k] = make_float2(offset_u[k], offset_v[k]);
+    }
+    if (!p->d_fspot) CTFP_CUDA(cudaMalloc(&p->d_fspot, sizeof(float2) * P));
+    CTFP_CUDA(cudaMemcpy(p->d_fspot, f.data(), sizeof(float2) * P, cudaMemcpyHostToDevice));
+    p->gp.fspot = p->d_fspot;
+    return CTFP_OK;
+}
+
+extern "C" ctfp_status ctfp_focal_spot_offsets(int64_t n_views, float focal_spot_size, float* offset_u,
+                                               float* offset_v)
+{
+    if (n_views < 0 || !offset_u || !offset_v) return fail(CTFP_INVALID_ARG, "bad argument");
+    if (!(focal_spot_size >= 0.f)) return fail(CTFP_INVALID_ARG, "focal_spot_size must be non-negative");
+    // CBCTForwardProj::computeFoSpOffset (CBCTForwardProj.cpp:122-148): srand(10),
+    // MSVC rand() (state * 214013 + 2531011, bits 16-30), offsets on a 1e-4 mm
+    // lattice across the spot [-r, r), redrawn while u^2 + v^2 > pi * r^2 (the
+    // reference's test: pi r^2, not r^2)
+    uint32_t state = 10u;
+    auto next = [&state]() {
+        state = state * 214013u + 2531011u;
+        return (int)((state >> 16) & 0x7fffu);
+    };
+    const float radius = focal_spot_size / 2.0f;
+    const int size = (int)(focal_spot_size * 10000);
+    const float pi = acosf(-1.0f);
+    for (int64_t k = 0; k < n_views; k++) {
+        float du = 0.f, dv = 0.f;
+        if (size > 0) {
+            const float bound = pi * radius * radius;
+            do {
+                du = -radius + (float)(next() % size) / 10000.0f;
+                dv = -radius + (float)(next() % size) / 10000.0f;
+            } while (du * du + dv * dv > bound);
+        }
+        offset_u[k] = du;
+        offset_v[k] = dv;
+    }
+    return CTFP_OK;
+}
 
 extern "C" ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* p, int32_t enable)
 {

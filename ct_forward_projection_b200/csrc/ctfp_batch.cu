@@ -430,7 +430,7 @@ struct DevScope {
 
 bool batchable(const ctfp_plan* p)
 {
-    return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_LAYERED;
+    return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_LAYERED && !plan_geom(p).fspot;
 }
 
 // Fills the per-call tables from the plans' current state.
@@ -440,7 +440,7 @@ ctfp_status fill_items(ctfp_batch* b)
         ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
         if (!batchable(p))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler");
+                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler and no focal spot");
         if (plan_energies(p) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
         ItemDesc& it = b->items[(size_t)s];
         const long long unit0 = it.unit0, units = it.units;
@@ -482,7 +482,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         if (plan_device(plans[i]) != dev) return bfail(CTFP_INVALID_ARG, "plans must share one device");
         if (!batchable(plans[i]))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler");
+                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler and no focal spot");
         if (plan_energies(plans[i]) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
     }
     DevScope ds(dev);

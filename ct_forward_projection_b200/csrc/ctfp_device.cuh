@@ -32,6 +32,7 @@ struct GeomParams {
     float pHalfX, pHalfY, pHalfZ, pSizeX, pSizeY, pSizeZ;
     const double2* trig;     // per view (cos, sin) of the FP32 view angle
     const float2* trigf;     // the same, rounded to FP32 (compat samplers)
+    const float2* fspot;     // per view focal-spot offset (u, v) in mm, or null
 };
 
 // One ray's sample segment: coordinates c(i) = a + b*i in FP64, evaluated
@@ -78,10 +79,18 @@ __device__ __forceinline__ RaySeg ray_segment(const GeomParams& g, int p, int v,
     const double t0 = sod - (double)g.FOVR + (double)g.dx / 2, dt = g.dx;  // .cu:1846
     const double2 cs = g.trig[p];
     const double cth = cs.x, sth = cs.y;
+    // focal-spot offset: added to the rotated y and the z coordinate
+    // (transformFocalSpotKernel, CBCTPolyProjGPU.cu:1943-1944)
+    double fu = 0.0, fv = 0.0;
+    if (g.fspot) {
+        const float2 f = g.fspot[p];
+        fu = f.x;
+        fv = f.y;
+    }
     // tu = X cos - Y sin + pHalfX; tv = -(X sin + Y cos) + pHalfY; tw = -Z + pHalfZ
     const double ku = A * cth - B * sth, cu = -sod * cth + (double)g.pHalfX;
-    const double kv = -(A * sth + B * cth), cv = sod * sth + (double)g.pHalfY;
-    const double kw = -C, cw = (double)g.pHalfZ;
+    const double kv = -(A * sth + B * cth), cv = sod * sth + (double)g.pHalfY + fu;
+    const double kw = -C, cw = (double)g.pHalfZ + fv;
     const double ax = (ku * t0 + cu) / g.pSizeX, bx = ku * dt / g.pSizeX;
     const double ay = (kv * t0 + cv) / g.pSizeY, by = kv * dt / g.pSizeY;
     const double az = (kw * t0 + cw) / g.pSizeZ, bz = kw * dt / g.pSizeZ;
@@ -112,6 +121,7 @@ struct RayRef32 {
     float cgcb, cgsb, sinG;  // direction cosines (.cu:1825-1829, 1846-1848)
     float c, s;              // cos, sin of the view angle
     float t0;                // sod - FOVR + dx / 2
+    float fu, fv;            // focal-spot offset of the view (0 without one), mm
 };
 
 __device__ __forceinline__ RayRef32 ray_ref32(const GeomParams& g, int p, int v, int u)
@@ -132,6 +142,13 @@ __device__ __forceinline__ RayRef32 ray_ref32(const GeomParams& g, int p, int v,
     r.c = cs.x;
     r.s = cs.y;
     r.t0 = __fadd_rn(__fsub_rn(g.sod, g.FOVR), __fdiv_rn(g.dx, 2.0f));
+    r.fu = 0.f;
+    r.fv = 0.f;
+    if (g.fspot) {
+        const float2 f = g.fspot[p];
+        r.fu = f.x;
+        r.fv = f.y;
+    }
     return r;
 }
 
@@ -143,8 +160,10 @@ __device__ __forceinline__ float3 ref32_coords(const GeomParams& g, const RayRef
     const float Y = __fmul_rn(r.cgsb, t);
     const float Z = __fmul_rn(r.sinG, t);
     const float tu = __fadd_rn(__fmaf_rn(X, r.c, -__fmul_rn(Y, r.s)), g.pHalfX);
-    const float tv = __fadd_rn(-__fmaf_rn(X, r.s, __fmul_rn(Y, r.c)), g.pHalfY);
-    const float tw = __fadd_rn(-Z, g.pHalfZ);
+    // + the focal-spot offset, added last as in CBCTPolyProjGPU.cu:1943-1944
+    // (adding 0 leaves the coordinate unchanged)
+    const float tv = __fadd_rn(__fadd_rn(-__fmaf_rn(X, r.s, __fmul_rn(Y, r.c)), g.pHalfY), r.fu);
+    const float tw = __fadd_rn(__fadd_rn(-Z, g.pHalfZ), r.fv);
     return make_float3(__fadd_rn(__fdiv_rn(tu, g.pSizeX), 0.5f), __fadd_rn(__fdiv_rn(tv, g.pSizeY), 0.5f),
                        __fadd_rn(__fdiv_rn(tw, g.pSizeZ), 0.5f));
 }

@@ -753,6 +753,92 @@ __global__ void k_occupancy(const VolPtrs vol, int M, int nx, int ny, int nz, in
 
 }  // namespace
 
+namespace {
+
+// Focal-spot re-alignment of the line-integral images (projOffsetMatchKernel,
+// CBCTPolyProjGPU.cu:1956-1978): out[p][v][u][m] = in[p] sampled at
+// (u + offU[p] / dSize, v + offV[p] / dSize), bilinear, 0 outside the image.
+// The compat modes reproduce the texture unit (8-bit weights at the FP32
+// coordinate u + offU/dSize + 0.5 it receives); TRILINEAR interpolates
+// exactly at the FP64 position.
+template <int M, int MODE>
+__global__ void k_shift_views(const float* __restrict__ in, float* __restrict__ out, const float2* __restrict__ fspot,
+                              int U, int V, float dSize, int view0, int n_views)
+{
+    const int64_t npix = (int64_t)U * V;
+    const int64_t n = npix * n_views;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / npix, pix = t % npix;
+        const int u = (int)(pix % U), v = (int)(pix / U);
+        const float2 f = fspot[view0 + k];
+        int ix, iy;
+        float w[4];  // (ix, iy), (ix + 1, iy), (ix, iy + 1), (ix + 1, iy + 1)
+        if (MODE == INTERP_TRILINEAR) {
+            const double cx = (double)u + (double)f.x / (double)dSize, cy = (double)v + (double)f.y / (double)dSize;
+            const double fx = floor(cx), fy = floor(cy);
+            ix = (int)fx;
+            iy = (int)fy;
+            float wx, ux, wy, uy;
+            frac_pair(cx - fx, wx, ux);
+            frac_pair(cy - fy, wy, uy);
+            w[0] = ux * uy; w[1] = wx * uy; w[2] = ux * wy; w[3] = wx * wy;
+        } else {
+            const float x = __fadd_rn(__fadd_rn((float)u, __fdiv_rn(f.x, dSize)), 0.5f);
+            const float y = __fadd_rn(__fadd_rn((float)v, __fdiv_rn(f.y, dSize)), 0.5f);
+            const int X = tex_fixed(x), Y = tex_fixed(y);
+            ix = X >> 8;
+            iy = Y >> 8;
+            float w8[8];
+            texunit_weights(X & 255, Y & 255, 0, w8);  // the view coordinate p + 0.5 has fraction 0
+            w[0] = w8[0]; w[1] = w8[1]; w[2] = w8[2]; w[3] = w8[3];
+        }
+        const float* src = in + k * npix * M;
+        float acc[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) acc[m] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int x = ix + (c & 1), y = iy + (c >> 1);
+            if ((unsigned)x >= (unsigned)U || (unsigned)y >= (unsigned)V) continue;
+            const float* q = src + ((int64_t)y * U + x) * M;
+#pragma unroll
+            for (int m = 0; m < M; m++) acc[m] = fmaf(w[c], __ldg(q + m), acc[m]);
+        }
+        float* d = out + t * M;
+#pragma unroll
+        for (int m = 0; m < M; m++) d[m] = acc[m];
+    }
+}
+
+template <int MODE>
+cudaError_t shift_dispatch(int M, const float* in, float* out, const float2* fspot, int U, int V, float dSize,
+                           int view0, int n_views, unsigned nb, cudaStream_t st)
+{
+    switch (M) {
+        case 1: k_shift_views<1, MODE><<<nb, 256, 0, st>>>(in, out, fspot, U, V, dSize, view0, n_views); break;
+        case 2: k_shift_views<2, MODE><<<nb, 256, 0, st>>>(in, out, fspot, U, V, dSize, view0, n_views); break;
+        case 3: k_shift_views<3, MODE><<<nb, 256, 0, st>>>(in, out, fspot, U, V, dSize, view0, n_views); break;
+        case 4: k_shift_views<4, MODE><<<nb, 256, 0, st>>>(in, out, fspot, U, V, dSize, view0, n_views); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_shift_views(const float* in, float* out, const GeomParams& g, int M, int interp, int view0,
+                               int n_views, cudaStream_t st)
+{
+    if (!g.fspot) return cudaErrorInvalidValue;
+    const int64_t n = (int64_t)g.U * g.V * n_views;
+    if (n == 0) return cudaSuccess;
+    int64_t nb = (n + 255) / 256;
+    if (nb > 148 * 32) nb = 148 * 32;
+    if (interp == INTERP_TRILINEAR)
+        return shift_dispatch<INTERP_TRILINEAR>(M, in, out, g.fspot, g.U, g.V, g.dSize, view0, n_views, (unsigned)nb, st);
+    return shift_dispatch<INTERP_TEXEMU>(M, in, out, g.fspot, g.U, g.V, g.dSize, view0, n_views, (unsigned)nb, st);
+}
+
 cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st)
 {
     const int ox = occ_dim(nx), oy = occ_dim(ny), oz = occ_dim(nz);

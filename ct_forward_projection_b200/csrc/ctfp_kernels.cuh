@@ -61,6 +61,10 @@ cudaError_t launch_finalize(int64_t n_pix, int64_t n_views, const float* I, cons
 cudaError_t launch_sample_points(const float* vol, cudaTextureObject_t tex, int nx, int ny, int nz, int interp,
                                  const float* pts, int64_t n, float* out, cudaStream_t st);
 cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, cudaStream_t st);
+// Focal-spot re-alignment of compact line-integral images [n_views][V][U][M]
+// of views view0.. (interp selects exact or texture-unit bilinear weights).
+cudaError_t launch_shift_views(const float* in, float* out, const GeomParams& g, int M, int interp, int view0,
+                               int n_views, cudaStream_t st);
 // Fills occ [occ_dim(nz)][occ_dim(ny)][occ_dim(nx)] from the M volumes
 // (vol: host array of M device pointers; occ is zeroed first).
 cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st);

@@ -118,6 +118,16 @@ class Projector:
         call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED,
                                                  "brick": capi.SAMPLER_BRICK}[sampler])
 
+    def set_focal_spot(self, offset_u=None, offset_v=None) -> None:
+        """Per-view focal-spot offsets in mm (ctfp_plan_set_focal_spot); None clears."""
+        if offset_u is None:
+            call("ctfp_plan_set_focal_spot", self._h, None, None)
+            return
+        u = np.ascontiguousarray(offset_u, dtype=np.float32)
+        v = np.ascontiguousarray(offset_v, dtype=np.float32)
+        assert u.shape == v.shape == (self.shape_proj[0],), "one offset pair per view"
+        call("ctfp_plan_set_focal_spot", self._h, _np_ptr(u), _np_ptr(v))
+
     def set_skip_empty(self, enable: bool = True) -> None:
         """Empty-space skipping for the layered sampler (ctfp_plan_set_skip_empty)."""
         call("ctfp_plan_set_skip_empty", self._h, 1 if enable else 0)
@@ -360,6 +370,14 @@ def sample_volume(volume, points, interp: str, stream=None):
     call("ctfp_sample_volume", _dptr(volume), nx, ny, nz, INTERP[interp], _dptr(points.contiguous()),
          points.shape[0], _dptr(out), _stream(stream))
     return out
+
+
+def focal_spot_offsets(n_views: int, focal_spot_size: float) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's per-view focal-spot offsets (ctfp_focal_spot_offsets), mm."""
+    u = np.empty(int(n_views), np.float32)
+    v = np.empty(int(n_views), np.float32)
+    call("ctfp_focal_spot_offsets", int(n_views), float(focal_spot_size), _np_ptr(u), _np_ptr(v))
+    return u, v
 
 
 def sampler_peak(device: int = 0, kind: str = "layered") -> float:

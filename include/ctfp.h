@@ -142,6 +142,24 @@ ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t 
  * one march every sample.  No counterpart in the reference. */
 ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* plan, int32_t enable);
 
+/* Focal spot (CBCTSinMatPolyForwardProj{Grid,NoGrid}::computePolyForwProjFoSp,
+ * Source/CBCTSinMatPolyForwardProjGrid.cpp:269-388, CBCTPolyProjGPU.cu:1927-1978):
+ * per-view source offsets offset_u, offset_v [projNum] in mm (host arrays,
+ * copied; both NULL clears).  The forward then samples each view with its
+ * offset added to the rotated y and the z coordinate, re-aligns the view's
+ * line-integral images by (offset_u, offset_v) / dSize detector pixels with
+ * bilinear interpolation (texture-unit weights in the compat modes, exact in
+ * CTFP_INTERP_TRILINEAR; 0 outside the image), and runs the spectral epilogue
+ * on the re-aligned integrals; an L checkpoint holds the re-aligned integrals.
+ * The reference's path exists for single-material phantoms; here every
+ * material is re-aligned alike.  The adjoint (ctfp_backward*) and the batched
+ * form return CTFP_UNSUPPORTED while a focal spot is set. */
+ctfp_status ctfp_plan_set_focal_spot(ctfp_plan* plan, const float* offset_u, const float* offset_v);
+/* The reference's offsets: srand(10), MSVC rand(), a 1e-4 mm lattice over
+ * [-size/2, size/2), redrawn while u^2 + v^2 > pi * (size/2)^2
+ * (CBCTForwardProj::computeFoSpOffset, Source/CBCTForwardProj.cpp:122-148). */
+ctfp_status ctfp_focal_spot_offsets(int64_t n_views, float focal_spot_size, float* offset_u, float* offset_v);
+
 /* Spectral tables, host pointers, copied into the plan.
  *   spectrum     [E]     normalised spectrum S_e
  *   mu           [E][M]  per-material attenuation per unit density, 1/mm per

@@ -98,7 +98,7 @@ typedef struct ray_coef {
 } ray_coef;
 
 static void ray_setup(const orc_geometry* g, const orc_sysinfo* s, double cth, double sth, int64_t v,
-                      int64_t u, ray_coef* r)
+                      int64_t u, double fu, double fv, ray_coef* r)
 {
     double dsz = g->dSize, sdd = g->sdd, sod = g->sod;
     double detU = (double)s->dHalfLU - dsz / 2 - (double)u * dsz;
@@ -112,8 +112,10 @@ static void ray_setup(const orc_geometry* g, const orc_sysinfo* s, double cth, d
     double t0 = sod - (double)s->FOVR + (double)s->dx / 2, dt = s->dx;
     /* tu = X cos - Y sin + pHalfX ; tv = -(X sin + Y cos) + pHalfY ; tw = -Z + pHalfZ */
     double ku = A * cth - B * sth, cu = -sod * cth + s->pHalfX;
-    double kv = -(A * sth + B * cth), cv = sod * sth + s->pHalfY;
-    double kw = -C, cw = s->pHalfZ;
+    /* fu, fv: focal-spot offset of the view, added to the rotated y and to z
+     * (transformFocalSpotKernel, CBCTPolyProjGPU.cu:1943-1944); 0 without one */
+    double kv = -(A * sth + B * cth), cv = sod * sth + s->pHalfY + fu;
+    double kw = -C, cw = s->pHalfZ + fv;
     r->ax = (ku * t0 + cu) / s->pSizeX;
     r->bx = ku * dt / s->pSizeX;
     r->ay = (kv * t0 + cv) / s->pSizeY;
@@ -131,6 +133,7 @@ static void ray_setup(const orc_geometry* g, const orc_sysinfo* s, double cth, d
  * reference's own FP32 arithmetic reproduces its outputs there. */
 typedef struct ray_ref32 {
     float cgcb, cgsb, sinG, c, s, t0;
+    float fu, fv; /* focal-spot offset, added last (CBCTPolyProjGPU.cu:1943-1944) */
 } ray_ref32;
 
 /* The products that the reference's nvcc build fuses into the following
@@ -152,6 +155,8 @@ static void ref32_setup(const orc_geometry* g, const orc_sysinfo* s, float angle
     r->c = (float)cos((double)angle);
     r->s = (float)sin((double)angle);
     r->t0 = (g->sod - s->FOVR) + s->dx / 2.0f;
+    r->fu = 0.0f;
+    r->fv = 0.0f;
 }
 
 static void ref32_coords(const orc_geometry* g, const orc_sysinfo* s, const ray_ref32* r, int64_t i, float* x)
@@ -159,8 +164,8 @@ static void ref32_coords(const orc_geometry* g, const orc_sysinfo* s, const ray_
     float t = fmaf((float)i, s->dx, r->t0);
     float X = fmaf(r->cgcb, t, -g->sod), Y = r->cgsb * t, Z = r->sinG * t;
     float tu = fmaf(X, r->c, -(Y * r->s)) + s->pHalfX;
-    float tv = -fmaf(X, r->s, Y * r->c) + s->pHalfY;
-    float tw = -Z + s->pHalfZ;
+    float tv = (-fmaf(X, r->s, Y * r->c) + s->pHalfY) + r->fu;
+    float tw = (-Z + s->pHalfZ) + r->fv;
     x[0] = tu / s->pSizeX + 0.5f;
     x[1] = tv / s->pSizeY + 0.5f;
     x[2] = tw / s->pSizeZ + 0.5f;
@@ -268,8 +273,8 @@ static void ray_index(const orc_geometry* g, int64_t id, int64_t* p, int64_t* v,
 /* ------------------------------------------------------------------------ */
 /* A2-A5: L[r][m] = dx * sum_{i<K} interp(vol_m, c_i) for the rays listed in
  * ray_ids (NULL = all projNum*dNumV*dNumU rays in [p][v][u] order). */
-void orc_line_integrals(const orc_geometry* g, int M, const float* const* vols, int mode, int64_t nrays,
-                        const int64_t* ray_ids, double* L)
+static void line_integrals(const orc_geometry* g, int M, const float* const* vols, int mode, int64_t nrays,
+                           const int64_t* ray_ids, const float* off_u, const float* off_v, double* L)
 {
     orc_sysinfo s;
     orc_compute_paras(g, &s);
@@ -280,10 +285,13 @@ void orc_line_integrals(const orc_geometry* g, int M, const float* const* vols, 
         ray_index(g, ray_ids ? ray_ids[r] : r, &p, &v, &u);
         float ang = orc_view_angle(g, &s, p);
         double th = (double)ang;
+        const float fu = off_u ? off_u[p] : 0.0f, fv = off_v ? off_v[p] : 0.0f;
         ray_coef c;
-        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        ray_setup(g, &s, cos(th), sin(th), v, u, (double)fu, (double)fv, &c);
         ray_ref32 r32;
         ref32_setup(g, &s, ang, v, u, &r32);
+        r32.fu = fu;
+        r32.fv = fv;
         double acc[8] = {0};
         for (int64_t i = 0; i < K; i++) {
             tri t;
@@ -291,6 +299,90 @@ void orc_line_integrals(const orc_geometry* g, int M, const float* const* vols, 
             for (int m = 0; m < M; m++) acc[m] += sample(vols[m], nx, ny, nz, &t);
         }
         for (int m = 0; m < M; m++) L[r * M + m] = (double)s.dx * acc[m];
+    }
+}
+
+/* A2-A5: L[r][m] = dx * sum_{i<K} interp(vol_m, c_i) for the rays listed in
+ * ray_ids (NULL = all projNum*dNumV*dNumU rays in [p][v][u] order). */
+void orc_line_integrals(const orc_geometry* g, int M, const float* const* vols, int mode, int64_t nrays,
+                        const int64_t* ray_ids, double* L)
+{
+    line_integrals(g, M, vols, mode, nrays, ray_ids, NULL, NULL, L);
+}
+
+/* The same with per-view focal-spot offsets off_u, off_v [projNum] (mm):
+ * transformFocalSpotKernel (CBCTPolyProjGPU.cu:1927-1954). */
+void orc_line_integrals_focal_spot(const orc_geometry* g, int M, const float* const* vols, int mode, int64_t nrays,
+                                   const int64_t* ray_ids, const float* off_u, const float* off_v, double* L)
+{
+    line_integrals(g, M, vols, mode, nrays, ray_ids, off_u, off_v, L);
+}
+
+/* Focal-spot re-alignment (projOffsetMatchKernel, CBCTPolyProjGPU.cu:1956-1978):
+ * out[p][v][u][m] = in[p] interpolated at (u + off_u[p] / dSize,
+ * v + off_v[p] / dSize), 0 outside the [V][U] image.  TEXEMU: the texture
+ * unit's weights at the FP32 coordinate u + off/dSize + 0.5 it receives (the
+ * view coordinate p + 0.5 has fraction 0); TRILINEAR: exact bilinear. */
+void orc_shift_views(int mode, int64_t P, int64_t V, int64_t U, int M, float dSize, const float* off_u,
+                     const float* off_v, const double* in, double* out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < P; p++) {
+        for (int64_t v = 0; v < V; v++) {
+            for (int64_t u = 0; u < U; u++) {
+                int64_t ix, iy;
+                double w[4];
+                if (mode == ORC_TEXEMU) {
+                    float x = ((float)u + off_u[p] / dSize) + 0.5f;
+                    float y = ((float)v + off_v[p] / dSize) + 0.5f;
+                    int64_t X = tex_fixed(x), Y = tex_fixed(y);
+                    double w8[8];
+                    ix = X >> 8;
+                    iy = Y >> 8;
+                    texunit_weights((int)(X & 255), (int)(Y & 255), 0, w8);
+                    for (int k = 0; k < 4; k++) w[k] = w8[k];
+                } else {
+                    double cx = (double)u + (double)off_u[p] / (double)dSize;
+                    double cy = (double)v + (double)off_v[p] / (double)dSize;
+                    double fx = floor(cx), fy = floor(cy), a = cx - fx, b = cy - fy;
+                    ix = (int64_t)fx;
+                    iy = (int64_t)fy;
+                    w[0] = (1 - a) * (1 - b); w[1] = a * (1 - b); w[2] = (1 - a) * b; w[3] = a * b;
+                }
+                for (int m = 0; m < M; m++) {
+                    double acc = 0.0;
+                    for (int k = 0; k < 4; k++) {
+                        int64_t x = ix + (k & 1), y = iy + (k >> 1);
+                        if (x < 0 || y < 0 || x >= U || y >= V) continue;
+                        acc += w[k] * in[((p * V + y) * U + x) * M + m];
+                    }
+                    out[((p * V + v) * U + u) * M + m] = acc;
+                }
+            }
+        }
+    }
+}
+
+/* CBCTForwardProj::computeFoSpOffset (CBCTForwardProj.cpp:122-148): srand(10),
+ * MSVC rand(); offsets on a 1e-4 mm lattice over [-r, r), redrawn while
+ * u^2 + v^2 > pi r^2. */
+void orc_focal_spot_offsets(int64_t n, float size, float* off_u, float* off_v)
+{
+    uint32_t state = 10u;
+    const float radius = size / 2.0f, pi = acosf(-1.0f);
+    const int sz = (int)(size * 10000);
+    for (int64_t k = 0; k < n; k++) {
+        float du = 0.0f, dv = 0.0f;
+        if (sz > 0) {
+            do {
+                state = state * 214013u + 2531011u;
+                du = -radius + (float)((int)((state >> 16) & 0x7fffu) % sz) / 10000.0f;
+                state = state * 214013u + 2531011u;
+                dv = -radius + (float)((int)((state >> 16) & 0x7fffu) % sz) / 10000.0f;
+            } while (du * du + dv * dv > pi * radius * radius);
+        }
+        off_u[k] = du;
+        off_v[k] = dv;
     }
 }
 
@@ -380,7 +472,7 @@ void orc_backward(const orc_geometry* g, int M, int mode, int E, const float* mu
         float ang = orc_view_angle(g, &s, p);
         double th = (double)ang;
         ray_coef c;
-        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        ray_setup(g, &s, cos(th), sin(th), v, u, 0.0, 0.0, &c);
         ray_ref32 r32;
         ref32_setup(g, &s, ang, v, u, &r32);
         for (int64_t i = 0; i < K; i++) {
@@ -408,7 +500,7 @@ void orc_line_integrals_adjoint(const orc_geometry* g, int M, int mode, int64_t 
         float ang = orc_view_angle(g, &s, p);
         double th = (double)ang;
         ray_coef c;
-        ray_setup(g, &s, cos(th), sin(th), v, u, &c);
+        ray_setup(g, &s, cos(th), sin(th), v, u, 0.0, 0.0, &c);
         ray_ref32 r32;
         ref32_setup(g, &s, ang, v, u, &r32);
         for (int64_t i = 0; i < K; i++) {

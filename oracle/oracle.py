@@ -96,12 +96,44 @@ def _rays(d, ray_ids):
     return len(r), r
 
 
-def line_integrals(d: dict, vols, mode: int = TRILINEAR, ray_ids=None) -> np.ndarray:
+def line_integrals(d: dict, vols, mode: int = TRILINEAR, ray_ids=None, focal_spot=None) -> np.ndarray:
+    """focal_spot: (offset_u, offset_v) per view in mm, or None."""
     n, r = _rays(d, ray_ids)
     arr, keep = _vol_array(vols)
     L = np.empty((n, len(keep)), np.float64)
-    lib().orc_line_integrals(C.byref(geom(d)), len(keep), arr, mode, C.c_int64(n), _p(r), _p(L))
+    if focal_spot is None:
+        lib().orc_line_integrals(C.byref(geom(d)), len(keep), arr, mode, C.c_int64(n), _p(r), _p(L))
+    else:
+        fu, fv = _f32(focal_spot[0]), _f32(focal_spot[1])
+        lib().orc_line_integrals_focal_spot(C.byref(geom(d)), len(keep), arr, mode, C.c_int64(n), _p(r), _p(fu),
+                                            _p(fv), _p(L))
     return L
+
+
+def shift_views(d: dict, L, M: int, focal_spot, mode: int = TRILINEAR) -> np.ndarray:
+    """Focal-spot re-alignment of all views' line integrals L [P*V*U][M]."""
+    P, V, U = int(d["projNum"]), int(d["dNumV"]), int(d["dNumU"])
+    L = np.ascontiguousarray(L, dtype=np.float64).reshape(P * V * U, M)
+    out = np.empty_like(L)
+    fu, fv = _f32(focal_spot[0]), _f32(focal_spot[1])
+    lib().orc_shift_views(mode, C.c_int64(P), C.c_int64(V), C.c_int64(U), M, C.c_float(float(d["dSize"])), _p(fu),
+                          _p(fv), _p(L), _p(out))
+    return out
+
+
+def focal_spot_offsets(n: int, size: float):
+    u = np.empty(n, np.float32)
+    v = np.empty(n, np.float32)
+    lib().orc_focal_spot_offsets(C.c_int64(n), C.c_float(size), _p(u), _p(v))
+    return u, v
+
+
+def forward_focal_spot(d: dict, vols, mu, W, focal_spot, mode: int = TRILINEAR) -> dict:
+    """The focal-spot forward: shifted march, re-alignment, spectral epilogue."""
+    M = len(vols)
+    L = shift_views(d, line_integrals(d, vols, mode, focal_spot=focal_spot), M, focal_spot, mode)
+    I, A = spectral(d, mu, W, L)
+    return {"I": I, "IAbsorb": A, "L": L}
 
 
 def energy_weights(d: dict, spectrum, grid=None, grid_layout: int = 0, det=None, I0Val: float = 1.0) -> np.ndarray:

@@ -291,3 +291,48 @@ def test_skip_empty_isolated_voxels_at_brick_edges(cuda_ok, pos):
     assert np.count_nonzero(full) > 0
     np.testing.assert_array_equal(skip != 0, full != 0)
     assert rel_err_scaled(skip, full) < 1e-6
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("M", [1, 2])
+def test_focal_spot_forward_vs_oracle(cuda_ok, mode, M):
+    from ct_forward_projection_b200.projector import focal_spot_offsets
+    d = small_geometry(n=(20, 18, 14), views=6, U=23, V=15)
+    vols = random_volumes(d, M, 70 + M)
+    S, mu, G, D = spectral_setup(d, M, 6, 5)
+    fs = focal_spot_offsets(d["projNum"], 1.2)  # up to ~1.3 detector pitches
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    omode = O.TRILINEAR if mode == "trilinear" else O.TEXEMU
+    ref = O.forward_focal_spot(d, vols, mu, W, fs, omode)
+    with Projector(d, M, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_focal_spot(*fs)
+        f = pr.forward(to_dev(vols), want_L=True)
+        L_only = pr.line_integrals(to_dev(vols))
+        torch.cuda.synchronize()
+    tol = RTOL_TRI if mode == "trilinear" else RTOL_TEX
+    assert rel_err(f["I"].cpu().numpy(), ref["I"]) < tol
+    assert rel_err(f["IAbsorb"].cpu().numpy(), ref["IAbsorb"]) < tol * 10
+    assert rel_err_scaled(f["L"].cpu().numpy().reshape(-1, M), ref["L"]) < tol
+    assert torch.equal(L_only, f["L"])
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu", "texture"])
+def test_focal_spot_zero_offsets_equal_plain_forward(cuda_ok, mode):
+    d = small_geometry(n=16, views=4, U=19, V=13)
+    vols = random_volumes(d, 2, 9)
+    S, mu, G, D = spectral_setup(d, 2, 5, 1)
+    with Projector(d, 2, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        a = pr.forward(to_dev(vols), want_L=True)
+        z = np.zeros(d["projNum"], np.float32)
+        pr.set_focal_spot(z, z)
+        b = pr.forward(to_dev(vols), want_L=True)
+        c = pr.forward(to_dev(vols), views=(1, 2))
+        with pytest.raises(Exception):
+            pr.backward(b["L"], gI=torch.ones_like(b["I"]))
+        pr.set_focal_spot(None)
+        torch.cuda.synchronize()
+    assert torch.equal(a["L"], b["L"])
+    assert rel_err(b["I"].cpu().numpy(), a["I"].cpu().numpy()) < 1e-6
+    assert rel_err(c["I"].cpu().numpy(), a["I"][1:3].cpu().numpy()) < 1e-6

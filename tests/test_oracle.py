@@ -153,3 +153,63 @@ def test_finalize_floor_and_log():
     assert Ip.tolist() == [[[10, 0]]]
     assert proj[0, 0, 0] == pytest.approx(np.log(2.0), rel=1e-6)
     assert np.isinf(proj[0, 0, 1])
+
+
+def _msvc_offsets(n, size):
+    # restatement of CBCTForwardProj::computeFoSpOffset in numpy float32
+    state = 10
+    r = np.float32(size / 2.0)
+    sz = int(np.float32(size) * np.float32(10000))
+    bound = np.float32(np.arccos(np.float32(-1.0))) * r * r
+
+    def rnd():
+        nonlocal state
+        state = (state * 214013 + 2531011) & 0xFFFFFFFF
+        return (state >> 16) & 0x7FFF
+
+    us, vs = [], []
+    for _ in range(n):
+        while True:
+            du = -r + np.float32(rnd() % sz) / np.float32(10000.0)
+            dv = -r + np.float32(rnd() % sz) / np.float32(10000.0)
+            if not (du * du + dv * dv > bound):
+                break
+        us.append(du)
+        vs.append(dv)
+    return np.array(us, np.float32), np.array(vs, np.float32)
+
+
+@pytest.mark.parametrize("size", [0.4, 1.0, 0.0123])
+def test_focal_spot_offsets_restatements_agree(size):
+    # the oracle's C restatement, the library's and a numpy restatement of the
+    # reference's srand(10) / MSVC rand() draw
+    from ct_forward_projection_b200.projector import focal_spot_offsets
+    u, v = O.focal_spot_offsets(300, size)
+    lu, lv = focal_spot_offsets(300, size)
+    nu, nv = _msvc_offsets(300, size)
+    np.testing.assert_array_equal(u, lu)
+    np.testing.assert_array_equal(v, lv)
+    np.testing.assert_array_equal(u, nu)
+    np.testing.assert_array_equal(v, nv)
+    r = size / 2
+    assert np.all(u >= -r - 1e-6) and np.all(u < r + 1e-6)
+    assert np.all(u * u + v * v <= np.pi * r * r + 1e-6)
+
+
+def test_shift_views_integer_offsets_move_the_image():
+    # an offset of exactly k detector pitches moves the image by k pixels,
+    # zero-filled at the edge, in both weight modes
+    d = dict(pNumX=4, pNumY=4, pNumZ=4, pLengthX=4.0, pLengthY=4.0, pLengthZ=4.0, projNum=2, dNumU=6, dNumV=5,
+             dSize=0.5, sod=100.0, sdd=200.0, rotatedDirection=1)
+    rng = np.random.RandomState(0)
+    L = rng.uniform(0, 1, (2, 5, 6, 2))
+    fu = np.array([1.0, -0.5], np.float32)  # +2 and -1 pixels
+    fv = np.array([0.0, 0.5], np.float32)   # 0 and +1 pixel
+    for mode in (O.TRILINEAR, O.TEXEMU):
+        out = O.shift_views(d, L.reshape(-1, 2), 2, (fu, fv), mode).reshape(2, 5, 6, 2)
+        ref0 = np.zeros_like(L[0])
+        ref0[:, :4] = L[0][:, 2:]
+        ref1 = np.zeros_like(L[1])
+        ref1[:4, 1:] = L[1][1:, :5]
+        np.testing.assert_array_equal(out[0], ref0)
+        np.testing.assert_array_equal(out[1], ref1)
