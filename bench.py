@@ -151,12 +151,13 @@ def cpu_baseline(w, gpu_I, budget_s: float):
     vols = [v.cpu().numpy() for v in w._vols]
     W = w._W
     mu = w.mu_table()
-    # calibrate on a small subset, then size the sample to the budget
-    ids = np.sort(rng.choice(n_rays, 512, replace=False))
+    # warm the thread pool, calibrate on a subset, then size the sample to the budget
+    O.forward(g, vols, mu, W, O.TRILINEAR, np.sort(rng.choice(n_rays, 512, replace=False)))
+    ids = np.sort(rng.choice(n_rays, 8192, replace=False))
     t0 = time.perf_counter()
     O.forward(g, vols, mu, W, O.TRILINEAR, ids)
     dt = time.perf_counter() - t0
-    n = int(min(n_rays, max(512, 512 * budget_s / max(dt, 1e-6))))
+    n = int(min(n_rays, max(8192, 8192 * budget_s / max(dt, 1e-6))))
     ids = np.sort(rng.choice(n_rays, n, replace=False))
     t0 = time.perf_counter()
     ref = O.forward(g, vols, mu, W, O.TRILINEAR, ids)
