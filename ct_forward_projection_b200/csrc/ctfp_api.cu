@@ -5,6 +5,7 @@
 // weights W[E][V][U], flat field I0, attenuation table) and, in texture mode,
 // one cudaArray + texture object per material.  No call resets the device and
 // none exits: every failure is a ctfp_status plus a per-thread message.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -58,6 +59,11 @@ struct ctfp_plan {
     float* h2d_vol[kMaxM] = {};
     float* d2h_I = nullptr;
     float* d2h_IAbs = nullptr;
+    // ctfp_forward_host pipelining: results of finished view chunks go back
+    // on a second stream while later chunks are marched
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t chunk_done[16] = {};
+    cudaEvent_t copies_done = nullptr;
 };
 
 namespace {
@@ -440,6 +446,10 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->d_gexp[m]);
     cudaFree(p->d_occ);
+    for (cudaEvent_t& e : p->chunk_done)
+        if (e) cudaEventDestroy(e);
+    if (p->copies_done) cudaEventDestroy(p->copies_done);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     cudaFree(p->d_fspot);
     cudaFree(p->d_fs_raw);
     cudaFree(p->d_fs_L);
@@ -544,7 +554,8 @@ ctfp_status ctfp_line_integrals(ctfp_plan* p, const float* const* volumes, float
 // The fused forward over views [view0, view0 + n_views); outputs hold those
 // views from index 0 when compact, else are full [projNum] arrays.
 static ctfp_status forward_range(ctfp_plan* p, const float* const* volumes, int64_t view0, int64_t n_views,
-                                 bool compact, float* I, float* IAbsorb, float* I0, float* L_ckpt, void* stream)
+                                 bool compact, float* I, float* IAbsorb, float* I0, float* L_ckpt, void* stream,
+                                 bool prepare = true)
 {
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
     ctfp_status st = check_volumes(p, volumes);
@@ -562,8 +573,10 @@ static ctfp_status forward_range(ctfp_plan* p, const float* const* volumes, int6
     prm.view0 = (int)view0;
     prm.n_views = (int)n_views;
     prm.out_view0 = compact ? (int)view0 : 0;
-    st = prepare_volumes(p, volumes, s);
-    if (st != CTFP_OK) return st;
+    if (prepare) {
+        st = prepare_volumes(p, volumes, s);
+        if (st != CTFP_OK) return st;
+    }
     if (n_views > 0 && p->gp.fspot) {
         // focal spot: march, re-align the line-integral images, then the
         // spectral epilogue on the re-aligned integrals
@@ -620,18 +633,39 @@ ctfp_status ctfp_forward_host(ctfp_plan* p, const float* const* host_volumes, fl
         if (!p->h2d_vol[m]) CTFP_CUDA(cudaMalloc(&p->h2d_vol[m], nvox * sizeof(float)));
     if (!p->d2h_I) CTFP_CUDA(cudaMalloc(&p->d2h_I, nray * sizeof(float)));
     if (!p->d2h_IAbs) CTFP_CUDA(cudaMalloc(&p->d2h_IAbs, nray * sizeof(float)));
+    const int kChunks = (int)(sizeof(p->chunk_done) / sizeof(p->chunk_done[0]));
+    if (!p->copy_stream) CTFP_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : p->chunk_done)
+        if (!e) CTFP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!p->copies_done) CTFP_CUDA(cudaEventCreateWithFlags(&p->copies_done, cudaEventDisableTiming));
     const float* dv[kMaxM] = {};
     for (int m = 0; m < p->M; m++) {
         CTFP_CUDA(cudaMemcpyAsync(p->h2d_vol[m], host_volumes[m], nvox * sizeof(float), cudaMemcpyHostToDevice, s));
         dv[m] = p->h2d_vol[m];
     }
-    st = ctfp_forward(p, dv, p->d2h_I, p->d2h_IAbs, nullptr, nullptr, stream);
+    st = prepare_volumes(p, dv, s);
     if (st != CTFP_OK) return st;
-    CTFP_CUDA(cudaMemcpyAsync(host_I, p->d2h_I, nray * sizeof(float), cudaMemcpyDeviceToHost, s));
-    CTFP_CUDA(cudaMemcpyAsync(host_IAbsorb, p->d2h_IAbs, nray * sizeof(float), cudaMemcpyDeviceToHost, s));
+    // the views in up to kChunks contiguous chunks: chunk c's results are
+    // copied back on the copy stream while chunk c + 1 is marched
+    const int64_t P = p->geom.projNum, npix = p->geom.dNumU * p->geom.dNumV;
+    const int64_t per = (P + kChunks - 1) / kChunks;
+    int c = 0;
+    for (int64_t v0 = 0; v0 < P; v0 += per, c++) {
+        const int64_t n = std::min(per, P - v0);
+        st = forward_range(p, dv, v0, n, false, p->d2h_I, p->d2h_IAbs, nullptr, nullptr, stream, false);
+        if (st != CTFP_OK) return st;
+        CTFP_CUDA(cudaEventRecord(p->chunk_done[c], s));
+        CTFP_CUDA(cudaStreamWaitEvent(p->copy_stream, p->chunk_done[c], 0));
+        const size_t off = (size_t)(v0 * npix), bytes = (size_t)(n * npix) * sizeof(float);
+        CTFP_CUDA(cudaMemcpyAsync(host_I + off, p->d2h_I + off, bytes, cudaMemcpyDeviceToHost, p->copy_stream));
+        CTFP_CUDA(cudaMemcpyAsync(host_IAbsorb + off, p->d2h_IAbs + off, bytes, cudaMemcpyDeviceToHost,
+                                  p->copy_stream));
+    }
     if (host_I0)
-        CTFP_CUDA(cudaMemcpyAsync(host_I0, p->d_I0, sizeof(float) * (size_t)(p->geom.dNumU * p->geom.dNumV),
-                                  cudaMemcpyDeviceToHost, s));
+        CTFP_CUDA(cudaMemcpyAsync(host_I0, p->d_I0, sizeof(float) * (size_t)npix, cudaMemcpyDeviceToHost,
+                                  p->copy_stream));
+    CTFP_CUDA(cudaEventRecord(p->copies_done, p->copy_stream));
+    CTFP_CUDA(cudaStreamWaitEvent(s, p->copies_done, 0));
     CTFP_CUDA(cudaStreamSynchronize(s));
     return CTFP_OK;
 }

@@ -194,10 +194,12 @@ ctfp_status ctfp_forward(ctfp_plan* plan, const float* const* volumes, float* I,
 
 /* ctfp_forward with HOST buffers, the shape of the reference's per-energy
  * launchers (CBCTPolyProjGPU.cu:12-109: host volume in, host I/IAbsorb out):
- * copies the M host volumes to plan-owned device buffers, runs ctfp_forward and
- * copies I, IAbsorb (host [projNum][dNumV][dNumU]) and I0 (host [dNumV][dNumU],
- * may be NULL) back, then synchronises the stream.  Page-locked host buffers
- * make the copies asynchronous DMA. */
+ * copies the M host volumes to plan-owned device buffers, runs the forward in
+ * up to 16 chunks of views and copies each chunk's I, IAbsorb (host
+ * [projNum][dNumV][dNumU]) back on a plan-owned stream while the next chunk is
+ * marched, then I0 (host [dNumV][dNumU], may be NULL), and synchronises the
+ * stream.  Page-locked host buffers make the copies asynchronous DMA (and let
+ * them overlap the march). */
 ctfp_status ctfp_forward_host(ctfp_plan* plan, const float* const* host_volumes, float* host_I,
                               float* host_IAbsorb, float* host_I0, void* stream);
 

@@ -175,15 +175,32 @@ def test_spectral_from_L_matches_fused(cuda_ok):
     assert torch.equal(f["I"], s["I"]) and torch.equal(f["IAbsorb"], s["IAbsorb"])
 
 
-def test_forward_host_matches_device(cuda_ok):
-    d = small_geometry()
+@pytest.mark.parametrize("views,pinned,focal", [(6, False, False), (13, True, False), (17, True, True),
+                                                 (3, False, True)])
+def test_forward_host_matches_device(cuda_ok, views, pinned, focal):
+    # ctfp_forward_host marches in view chunks whose results travel back on a
+    # second stream; pageable or page-locked host buffers, with and without a
+    # focal spot, give the device path's results exactly
+    d = small_geometry(views=views)
     vols = random_volumes(d, 2, 8)
     S, mu, G, D = spectral_setup(d, 2, 7, 3)
     with Projector(d, 2, "trilinear") as pr:
         pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        if focal:
+            from ct_forward_projection_b200.projector import focal_spot_offsets
+            pr.set_focal_spot(*focal_spot_offsets(views, 0.8))
         dev = pr.forward(to_dev(vols))
         torch.cuda.synchronize()
-        host = pr.forward_host(vols)
+        out = None
+        if pinned:
+            P, V, U = pr.shape_proj
+            out = {"I": torch.empty((P, V, U)).pin_memory(), "IAbsorb": torch.empty((P, V, U)).pin_memory(),
+                   "I0": torch.empty((V, U)).pin_memory()}
+            hv = [torch.from_numpy(v).pin_memory() for v in vols]
+        else:
+            hv = vols
+        host = pr.forward_host(hv, out=out)
+        host = {k: np.asarray(v) for k, v in host.items()}
     assert np.array_equal(host["I"], dev["I"].cpu().numpy())
     assert np.array_equal(host["IAbsorb"], dev["IAbsorb"].cpu().numpy())
     assert np.array_equal(host["I0"], dev["I0"].cpu().numpy())
