@@ -353,3 +353,17 @@ def test_focal_spot_zero_offsets_equal_plain_forward(cuda_ok, mode):
     assert torch.equal(a["L"], b["L"])
     assert rel_err(b["I"].cpu().numpy(), a["I"].cpu().numpy()) < 1e-6
     assert rel_err(c["I"].cpu().numpy(), a["I"][1:3].cpu().numpy()) < 1e-6
+
+
+def test_deep_volume_falls_back_to_global_sampler(cuda_ok):
+    # layered textures hold at most 2048 layers: a deeper volume is marched
+    # through the global sampler, and asking for the layered one is refused
+    from ct_forward_projection_b200._capi import CtfpError, CTFP_UNSUPPORTED
+    d = small_geometry(n=(6, 5, 2050), views=2, U=7, V=9, length=6.0, pitch=2.0)
+    vols = random_volumes(d, 1, 3)
+    with Projector(d, 1, "trilinear") as pr:
+        L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1, 1)
+        with pytest.raises(CtfpError) as e:
+            pr.set_sampler("layered")
+        assert e.value.status == CTFP_UNSUPPORTED
+    assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
