@@ -301,7 +301,7 @@ def main():
 
     # ---------------- optional empty-space skipping (not the headline) -------
     skip = None
-    if args.interp != "texture" and args.sampler == "layered":
+    if args.interp == "texture" or args.sampler == "layered":
         ref_I = out["I"].clone()
         pr.set_skip_empty(True)
         o2 = {"I": torch.empty_like(out["I"]), "IAbsorb": torch.empty_like(out["IAbsorb"])}

@@ -302,6 +302,8 @@ void CBCTForwardProj::runDeviceProjection(bool grid, bool response, bool single)
 
     PlanGuard plan;
     CTFP_CHECK(ctfp_plan_create(&g, M, interp_from_env(), 0, &plan.p));
+    if (const char* sk = std::getenv("CTFP_SKIP_EMPTY"))
+        if (sk[0] == '1') CTFP_CHECK(ctfp_plan_set_skip_empty(plan.p, 1));
     if (focalSpot_)
         CTFP_CHECK(ctfp_plan_set_focal_spot(plan.p, h_mForwardProj.foSpOffsetU, h_mForwardProj.foSpOffsetV));
     DeviceBuffers db;

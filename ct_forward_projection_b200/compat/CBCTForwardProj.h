@@ -13,6 +13,7 @@
 // The sampler follows the environment variable CTFP_INTERP: "texture"
 // (default: the reference's hardware tex3D), "texemu" (its exact software
 // emulation) or "trilinear" (exact FP32 trilinear at FP64 coordinates).
+// CTFP_SKIP_EMPTY=1 turns on empty-space skipping (ctfp_plan_set_skip_empty).
 #pragma once
 
 #include <filesystem>

@@ -69,6 +69,9 @@ __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, 
 #pragma unroll 2
         for (int i = s.i0; i < s.i1; i++) {
             const float3 x = ref32_coords(prm.g, r, i);
+            // with empty-space skipping: the unit's own footprint (base texel
+            // of its fixed-point coordinate) in an all-zero brick filters to 0
+            if (SAMPLER == SAMPLER_LAYERED_SKIP && !footprint_occupied(prm, corner_tex(x))) continue;
 #pragma unroll
             for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(prm.tex[m], x.x, x.y, x.z));
         }
@@ -569,6 +572,8 @@ cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, b
             return lay ? fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_LAYERED>(prm, spec, minb, grid, block, smem, st)
                        : fwd_dispatch_spec<M, INTERP_TEXEMU, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
         case INTERP_TEXTURE:
+            if (prm.occ)
+                return fwd_dispatch_spec<M, INTERP_TEXTURE, SAMPLER_LAYERED_SKIP>(prm, spec, minb, grid, block, smem, st);
             return fwd_dispatch_spec<M, INTERP_TEXTURE, SAMPLER_GLOBAL>(prm, spec, minb, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;

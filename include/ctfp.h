@@ -133,13 +133,14 @@ ctfp_status ctfp_plan_set_sampler(ctfp_plan* plan, int32_t sampler);
 ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,
                                        int32_t min_ctas_per_sm);
 
-/* Empty-space skipping for the layered sampler (CTFP_INTERP_TRILINEAR,
- * CTFP_INTERP_TEXEMU; off by default).  Each call first marks the 8^3-voxel
- * bricks (dilated by one voxel) that hold a non-zero voxel of any material;
- * the march then skips samples whose 2x2x2 footprint lies in an unmarked
- * brick, whose contribution is exactly zero.  Results equal the full march up
- * to FP32 rounding of the compensated sums.  Samplers other than the layered
- * one march every sample.  No counterpart in the reference. */
+/* Empty-space skipping (off by default) for the layered sampler
+ * (CTFP_INTERP_TRILINEAR, CTFP_INTERP_TEXEMU) and the hardware texture
+ * (CTFP_INTERP_TEXTURE).  Each call first marks the 8^3-voxel bricks (dilated
+ * by one voxel) that hold a non-zero voxel of any material; the march then
+ * skips samples whose 2x2x2 footprint lies in an unmarked brick, whose
+ * contribution is exactly zero.  Results equal the full march up to FP32
+ * rounding of the compensated sums.  The global and brick samplers march every
+ * sample.  No counterpart in the reference. */
 ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* plan, int32_t enable);
 
 /* Focal spot (CBCTSinMatPolyForwardProj{Grid,NoGrid}::computePolyForwProjFoSp,

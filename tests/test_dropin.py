@@ -108,3 +108,23 @@ def test_cli_files_match_reference_binary(fx, cuda_ok, tmp_path, name, interp):
     assert np.max(np.abs(proj[big] - rproj[big])) < 1e-3
     if (p + "out_ADetResponse") in fx.files:
         np.testing.assert_allclose(outs["ADetResponse"], fx[p + "out_ADetResponse"], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_cli_skip_empty_matches_reference_binary(fx, cuda_ok, tmp_path, name):
+    # CTFP_SKIP_EMPTY=1 (empty-space skipping in the hardware-texture march)
+    # writes the same files within the same bounds
+    case = case_from_fixture(fx, name)
+    ref_runner.write_case(str(tmp_path), case)
+    r = run_cli(str(tmp_path), {"CTFP_INTERP": "texture", "CTFP_SKIP_EMPTY": "1"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    outs = ref_runner.read_outputs(str(tmp_path), case)
+    p = name + "/"
+    if name == "test_i0":
+        return
+    for key in ("PhoImgPro", "PhoImgAbsorb"):
+        ref = fx[p + "out_" + key].astype(np.float64)
+        got = outs[key].astype(np.float64)
+        err = np.maximum(np.abs(got - ref) - 1.0, 0.0) / np.maximum(ref, 1.0)
+        assert np.max(err) < RTOL_COUNTS, (key, float(np.max(err)))

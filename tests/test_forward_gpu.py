@@ -270,7 +270,7 @@ def _sparse_volumes(d, M, seed):
     return vols
 
 
-@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("mode", ["trilinear", "texemu", "texture"])
 @pytest.mark.parametrize("M", [1, 2, 3])
 def test_skip_empty_matches_full_march(cuda_ok, mode, M):
     d = small_geometry(n=(40, 36, 30), views=6, U=37, V=29)
@@ -293,15 +293,16 @@ def test_skip_empty_matches_full_march(cuda_ok, mode, M):
         assert rel_err(skip["I"].cpu().numpy(), ref["I"]) < RTOL_TRI
 
 
+@pytest.mark.parametrize("mode", ["trilinear", "texture"])
 @pytest.mark.parametrize("pos", [(0, 0, 0), (6, 7, 8), (7, 15, 23), (8, 16, 24), (15, 9, 31), (31, 31, 31)])
-def test_skip_empty_isolated_voxels_at_brick_edges(cuda_ok, pos):
+def test_skip_empty_isolated_voxels_at_brick_edges(cuda_ok, pos, mode):
     # one non-zero voxel on either side of the 8-voxel brick boundaries and at
     # the volume's faces: a brick missed by the dilation would drop every ray
     # through that voxel's footprint
     d = small_geometry(n=32, views=5, U=41, V=41, pitch=0.9)
     vol = np.zeros((32, 32, 32), np.float32)
     vol[pos[2], pos[1], pos[0]] = 1.5
-    with Projector(d, 1, "trilinear") as pr:
+    with Projector(d, 1, mode) as pr:
         full = pr.line_integrals(to_dev([vol])).cpu().numpy()
         pr.set_skip_empty(True)
         skip = pr.line_integrals(to_dev([vol])).cpu().numpy()
