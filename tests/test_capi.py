@@ -4,6 +4,7 @@ import ctypes as C
 import glob
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -90,3 +91,40 @@ def test_no_gpu_plan_create_fails_loudly():
     st = capi.lib().ctfp_plan_create(C.byref(g), 1, 0, 0, C.byref(h))
     assert st in (capi.CTFP_CUDA_ERROR, capi.CTFP_OOM)
     assert not h.value
+
+
+C_SRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c_abi", "forward_host.c")
+
+
+def _build_c_example(tmp_path):
+    exe = str(tmp_path / "forward_host")
+    pkg = os.path.dirname(capi.LIB_PATH)
+    inc = os.path.join(os.path.dirname(pkg), "include")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", inc, C_SRC, "-o", exe, "-L", pkg,
+                        "-lctfp", f"-Wl,-rpath,{pkg}", "-lm"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_c_caller_compiles_against_the_header(tmp_path):
+    # the boundary is plain C: a C99 program builds against include/ctfp.h and links libctfp.so
+    assert os.access(_build_c_example(tmp_path), os.X_OK)
+
+
+@pytest.mark.gpu
+def test_c_caller_matches_python_mirror(tmp_path):
+    import numpy as np
+    exe = _build_c_example(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.array([[float(x) for x in line.split()] for line in r.stdout.strip().splitlines()], np.float32)
+    from ct_forward_projection_b200 import Projector
+    d = dict(pNumX=16, pNumY=14, pNumZ=12, pLengthX=16.0, pLengthY=14.0, pLengthZ=12.0, projNum=4, dNumU=20, dNumV=15,
+             dSize=1.6, sod=300.0, sdd=450.0, rotatedDirection=1)
+    rho = (0.5 + (np.arange(16 * 14 * 12) % 7) * 0.25).astype(np.float32).reshape(12, 14, 16)
+    with Projector(d, 1, "trilinear") as pr:
+        pr.set_spectral_tables(np.array([0.2, 0.5, 0.3], np.float32), np.array([[0.040], [0.025], [0.018]], np.float32),
+                               None, 0, None, 1000.0)
+        out = pr.forward_host([rho])
+    np.testing.assert_array_equal(got[:, 0], out["I"].ravel())
+    np.testing.assert_array_equal(got[:, 1], out["IAbsorb"].ravel())
