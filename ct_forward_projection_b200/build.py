@@ -59,11 +59,13 @@ def build_lib(force: bool = False) -> str:
         return LIB
     objdir = os.path.join(ROOT, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for s in srcs:
-        o = os.path.join(objdir, os.path.basename(s) + ".o")
-        _run([NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-dc", s, "-o", o])
-        objs.append(o)
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    # the translation units compile independently: in parallel, largest first
+    from concurrent.futures import ThreadPoolExecutor
+    jobs = sorted(zip(srcs, objs), key=lambda so: -os.path.getsize(so[0]))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, [NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-dc", s, "-o", o]) for s, o in jobs]:
+            f.result()
     _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
     return LIB
 
