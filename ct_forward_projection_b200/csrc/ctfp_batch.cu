@@ -3,7 +3,7 @@
 // device work queue, the whole call replayed as one CUDA graph.  No reference
 // counterpart.
 //
-// Work unit = (item, view, 16 x 8 pixel tile): the 128 rays of one CTA, whose
+// Work unit = (item, view, 8 x 8 pixel tile): the 64 rays of one CTA, whose
 // neighbouring rays share texture-cache lines.  Items are grouped by material
 // count and sampler mode (one kernel instantiation each, so every group runs
 // with the registers its own march needs); within a group they are queued
@@ -45,8 +45,10 @@ using namespace ctfp;
 
 namespace {
 
-constexpr int kTU = 16, kTV = 8;      // rays of one unit (one CTA): u x v
-constexpr int kWarps = 4, kThreads = 32 * kWarps;
+// rays of one unit (one CTA): u x v.  8 x 8 measured 3 % faster than 16 x 8
+// for the fused adjoint (more CTAs in flight per SM) and equal for the forward.
+constexpr int kTU = 8, kTV = 8;
+constexpr int kWarps = 2, kThreads = 32 * kWarps;
 
 // One item as the persistent kernels see it.  The pointer fields are refreshed
 // per call.
@@ -188,12 +190,12 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     return res * res;
 }
 
-// CTAs of 128 threads per SM the kernels are compiled for (their register
-// caps: 65536 / (128 * minb)); the fused adjoint carries the scatter's run
+// CTAs of 64 threads per SM the kernels are compiled for (their register
+// caps: 65536 / (64 * minb)); the fused adjoint carries the scatter's run
 // accumulators on top of the march.
 template <bool ADJOINT, int M>
 struct BatchBudget {
-    static constexpr int minb = ADJOINT ? (M <= 2 ? 5 : 4) : (M <= 2 ? 8 : 6);
+    static constexpr int minb = ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 16 : 12);
 };
 
 template <int M, int MODE, bool ADJOINT>

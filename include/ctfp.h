@@ -263,8 +263,8 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * No counterpart in the reference, which simulates one phantom per process run
  * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
  * spectral tables; one device) and runs them with persistent kernels over a
- * device work queue: a work unit is one view x one 16 x 8 detector tile (the
- * 128 rays of one CTA); items are grouped by material count and sampler mode
+ * device work queue: a work unit is one view x one 8 x 8 detector tile (the
+ * 64 rays of one CTA); items are grouped by material count and sampler mode
  * (one kernel per group, each with its own register budget) and queued
  * largest first (rays x samples x materials); every CTA takes the next unit
  * from an atomic counter.  A call is recorded once as a CUDA graph (volume

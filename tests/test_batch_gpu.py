@@ -1,5 +1,5 @@
 """The batched form (ctfp_batch_*; no reference counterpart): persistent
-kernels over a work queue of (item, view, 16 x 8 ray tile) units, replayed as
+kernels over a work queue of (item, view, 8 x 8 ray tile) units, replayed as
 a CUDA graph.  Every item's outputs must equal the plain per-plan calls on the same
 inputs; the fused forward + loss + adjoint must equal ctfp_forward followed by
 ctfp_backward with dLoss/dI formed on the host."""
@@ -45,7 +45,7 @@ def test_batch_forward_equals_plain_calls(cuda_ok):
     items = make_items(ITEMS)
     b = Batch([it[0] for it in items])
     info = b.info()
-    assert info["units"] == sum(((sp["U"] + 15) // 16) * ((sp["V"] + 7) // 8) * sp["views"] for sp in ITEMS)
+    assert info["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 7) // 8) * sp["views"] for sp in ITEMS)
     assert info["grid_forward"] % 148 == 0 and info["grid_adjoint"] % 148 == 0
     outs = b.forward([it[1] for it in items], want_L=True)
     torch.cuda.synchronize()
