@@ -140,9 +140,15 @@ def max_over_ranks(x: float, ws: int) -> float:
     return float(t.item())
 
 
-def cpu_baseline(w, gpu_I, budget_s: float):
+def _err_stats(x: np.ndarray) -> dict:
+    return {"max": float(np.max(x)), "p99": float(np.percentile(x, 99))}
+
+
+def cpu_baseline(w, gpu: dict, budget_s: float):
     """FP64 oracle over a seeded subset of rays on all host cores; also the
-    max relative error of the GPU result on those rays."""
+    error of the GPU result on those rays: per-ray relative error of I,
+    IAbsorb and I0 (max and 99th percentile) and the absolute error of the
+    compat projection log(I0 / floor(I)) (CBCTForwardProj.cpp:376-387)."""
     from oracle import oracle as O
     from ct_forward_projection_b200.projector import Projector  # noqa: F401  (tables below)
     g = w.geometry
@@ -152,20 +158,45 @@ def cpu_baseline(w, gpu_I, budget_s: float):
     W = w._W
     mu = w.mu_table()
     # warm the thread pool, calibrate on a subset, then size the sample to the budget
-    O.forward(g, vols, mu, W, O.TRILINEAR, np.sort(rng.choice(n_rays, 512, replace=False)))
-    ids = np.sort(rng.choice(n_rays, 8192, replace=False))
+    n0 = min(8192, n_rays)
+    O.forward(g, vols, mu, W, O.TRILINEAR, np.sort(rng.choice(n_rays, min(512, n_rays), replace=False)))
+    ids = np.sort(rng.choice(n_rays, n0, replace=False))
     t0 = time.perf_counter()
     O.forward(g, vols, mu, W, O.TRILINEAR, ids)
     dt = time.perf_counter() - t0
-    n = int(min(n_rays, max(8192, 8192 * budget_s / max(dt, 1e-6))))
+    n = int(min(n_rays, max(n0, n0 * budget_s / max(dt, 1e-6))))
     ids = np.sort(rng.choice(n_rays, n, replace=False))
     t0 = time.perf_counter()
     ref = O.forward(g, vols, mu, W, O.TRILINEAR, ids)
     dt = time.perf_counter() - t0
-    got = gpu_I.reshape(-1)[ids].astype(np.float64)
-    err = float(np.max(np.abs(got - ref["I"]) / np.maximum(np.abs(ref["I"]), 1e-30)))
-    return {"value": n / dt, "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{n} seeded random rays (seed 7) of the full workload, FP64 oracle, {dt:.1f} s"}, err
+    def rel(a, b):
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-30)
+
+    pix = ids % (g["dNumU"] * g["dNumV"])
+    got = {k: gpu[k].reshape(-1)[pix if k == "I0" else ids].astype(np.float64) for k in ("I", "IAbsorb", "I0")}
+    ref_I0 = ref["I0"].reshape(-1)[pix]
+    acc = {k: _err_stats(rel(got[k], r)) for k, r in (("I", ref["I"]), ("IAbsorb", ref["IAbsorb"]), ("I0", ref_I0))}
+    with np.errstate(divide="ignore"):
+        proj_got = np.log(got["I0"] / np.floor(got["I"]))
+        proj_ref = np.log(ref_I0 / np.floor(ref["I"]))
+    acc["proj_abs"] = _err_stats(np.abs(proj_got - proj_ref))
+    acc["proj_abs"]["note"] = "includes the floor to integer counts: I one count apart near an integer gives ~1/I"
+    acc["rays"] = n
+    cpu = {"value": n / dt, "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
+           "cpu_model": _cpu_model(),
+           "sample": f"{n} seeded random rays (seed 7) of the full workload, FP64 oracle, {dt:.1f} s"}
+    return cpu, acc
+
+
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def reference_arm(args, w, ws, rank):
@@ -420,11 +451,14 @@ def main():
 
     # ---------------- CPU baseline (rank 0, N = 1) --------------------------
     cpu = None
-    err = None
+    err = acc = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         w._vols = vols
         w._W = _weights_from_tables(w, local)
-        cpu, err = cpu_baseline(w, out["I"].cpu().numpy(), args.cpu_budget)
+        gpu = {k: out[k].cpu().numpy() for k in ("I", "IAbsorb")}
+        gpu["I0"] = pr.forward(vols, views=(0, 1))["I0"].cpu().numpy()  # view-independent; not in the timed step
+        cpu, acc = cpu_baseline(w, gpu, args.cpu_budget)
+        err = acc["I"]["max"]
 
     if rank == 0:
         line = {
@@ -444,6 +478,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "max_rel_err_vs_fp64_oracle": err,
+            "accuracy_vs_fp64_oracle": acc,
             "fwd_adjoint": fa,
             "fwd_skip_empty": skip,
             "batch": batch,
