@@ -10,6 +10,7 @@
 // mu_E-volume integral because trilinear interpolation is linear in the voxel
 // values), and the energy sum runs on the device in compensated FP32.
 #include <algorithm>
+#include <atomic>
 
 #include "ctfp_kernels.cuh"
 
@@ -510,15 +511,16 @@ __global__ void __launch_bounds__(kBU * kBV, MINB) k_forward_brick(const MarchPa
 template <int M, int MODE, bool SPEC>
 cudaError_t brick_launch(const MarchParams& prm, dim3 grid, size_t smem, cudaStream_t st)
 {
-    // the dynamic shared-memory opt-in is per device
-    static unsigned long long attr_set = 0;
+    // the dynamic shared-memory opt-in is per device; plans on other threads
+    // may get here at the same time (setting the attribute twice is harmless)
+    static std::atomic<unsigned long long> attr_set{0};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !(attr_set >> dev & 1ull)) {
+    if (dev >= 64 || !(attr_set.load() >> dev & 1ull)) {
         cudaError_t e = cudaFuncSetAttribute(k_forward_brick<M, MODE, SPEC, 4>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= 1ull << dev;
+        if (dev < 64) attr_set.fetch_or(1ull << dev);
     }
     k_forward_brick<M, MODE, SPEC, 4><<<grid, dim3(kBU, kBV), smem, st>>>(prm);
     return cudaGetLastError();
