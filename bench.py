@@ -57,9 +57,11 @@ def measured_peak_hbm():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling.  Started before the timed region
+    (and waited on until its first sample lands), it keeps only the samples
+    whose timestamps fall between begin() and end()."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -67,14 +69,24 @@ class ClockSampler:
         self.idx = gpu_index
         self.proc = None
         self.path = os.path.join("/tmp", f"ctfp_clocks_{os.getpid()}.csv")
+        self.t0 = self.t1 = None
 
     def start(self):
         if not shutil.which("nvidia-smi"):
             return
         self.f = open(self.path, "w")
         self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                      stderr=subprocess.DEVNULL)
+        deadline = time.time() + 3.0
+        while time.time() < deadline and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -85,23 +97,28 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        import datetime
+        rows = []
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if self.t0 is not None and self.t0 - 0.05 <= r[0] <= self.t1 + 0.05]
+        window = "timed region"
+        if not inside:
+            inside, window = rows, "whole run (no sample inside the timed region)"
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {n for r in inside for n, v in zip(names, r[3]) if v.lower() == "active"}
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[2] for r in inside) if inside else None,
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def dist_setup(n_gpus):
@@ -318,12 +335,14 @@ def main():
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier_sync(ws)
+    clocks.begin()
     for s in range(args.steps):
         flush.fill_(float(s))
         ev[s][0].record(stream)
         pr.forward(vols, out=out, views=vr)
         ev[s][1].record(stream)
     barrier_sync(ws)
+    clocks.end()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms = max_over_ranks(statistics.mean(step_ms), ws)

@@ -1,0 +1,52 @@
+"""Host logic of bench.py that needs no GPU: the clock sampler keeps only the
+nvidia-smi samples taken inside the timed region and reads the throttle
+reasons from them (a stand-in nvidia-smi on PATH prints the samples)."""
+import os
+import stat
+import sys
+import time
+
+import bench
+
+FAKE = """#!{python}
+import datetime, sys, time
+reason = "{reason}"
+while True:
+    now = datetime.datetime.now()
+    ts = now.strftime("%Y/%m/%d %H:%M:%S.") + "%03d" % (now.microsecond // 1000)
+    print(ts + ", 0, {mhz}, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, " + reason, flush=True)
+    time.sleep(0.05)
+"""
+
+
+def fake_smi(tmp_path, monkeypatch, mhz, reason):
+    p = tmp_path / "nvidia-smi"
+    p.write_text(FAKE.format(python=sys.executable, mhz=mhz, reason=reason))
+    p.chmod(p.stat().st_mode | stat.S_IEXEC)
+    monkeypatch.setenv("PATH", str(tmp_path) + os.pathsep + os.environ["PATH"])
+
+
+def test_clock_samples_inside_the_timed_region(tmp_path, monkeypatch):
+    fake_smi(tmp_path, monkeypatch, 1965, "Active")
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.3)  # samples before the timed region are left out
+    c.begin()
+    time.sleep(0.5)
+    c.end()
+    time.sleep(0.3)
+    r = c.stop()
+    assert r["window"] == "timed region"
+    assert 4 <= r["samples"] <= 14
+    assert r["sm_mhz"] == 1965.0 and r["sm_max_mhz"] == 1965.0
+    assert r["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_sampler_without_a_window_keeps_every_sample(tmp_path, monkeypatch):
+    fake_smi(tmp_path, monkeypatch, 1500, "Not Active")
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.3)
+    r = c.stop()
+    assert r["window"].startswith("whole run")
+    assert r["samples"] >= 1 and r["sm_mhz"] == 1500.0 and r["reasons"] == []
