@@ -60,8 +60,12 @@ struct ctfp_plan {
     float* d2h_I = nullptr;
     float* d2h_IAbs = nullptr;
     // ctfp_forward_host pipelining: results of finished view chunks go back
-    // on a second stream while later chunks are marched
+    // on a second stream while later chunks are marched; the chunks alternate
+    // between the caller's stream and march_stream, so each chunk's last wave
+    // of CTAs overlaps the next chunk's first
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t march_stream = nullptr;
+    cudaEvent_t prepared = nullptr;
     cudaEvent_t chunk_done[16] = {};
     cudaEvent_t copies_done = nullptr;
 };
@@ -449,7 +453,9 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     for (cudaEvent_t& e : p->chunk_done)
         if (e) cudaEventDestroy(e);
     if (p->copies_done) cudaEventDestroy(p->copies_done);
+    if (p->prepared) cudaEventDestroy(p->prepared);
     if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    if (p->march_stream) cudaStreamDestroy(p->march_stream);
     cudaFree(p->d_fspot);
     cudaFree(p->d_fs_raw);
     cudaFree(p->d_fs_L);
@@ -635,9 +641,11 @@ ctfp_status ctfp_forward_host(ctfp_plan* p, const float* const* host_volumes, fl
     if (!p->d2h_IAbs) CTFP_CUDA(cudaMalloc(&p->d2h_IAbs, nray * sizeof(float)));
     const int kChunks = (int)(sizeof(p->chunk_done) / sizeof(p->chunk_done[0]));
     if (!p->copy_stream) CTFP_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    if (!p->march_stream) CTFP_CUDA(cudaStreamCreateWithFlags(&p->march_stream, cudaStreamNonBlocking));
     for (cudaEvent_t& e : p->chunk_done)
         if (!e) CTFP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (!p->copies_done) CTFP_CUDA(cudaEventCreateWithFlags(&p->copies_done, cudaEventDisableTiming));
+    if (!p->prepared) CTFP_CUDA(cudaEventCreateWithFlags(&p->prepared, cudaEventDisableTiming));
     const float* dv[kMaxM] = {};
     for (int m = 0; m < p->M; m++) {
         CTFP_CUDA(cudaMemcpyAsync(p->h2d_vol[m], host_volumes[m], nvox * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -646,17 +654,40 @@ ctfp_status ctfp_forward_host(ctfp_plan* p, const float* const* host_volumes, fl
     st = prepare_volumes(p, dv, s);
     if (st != CTFP_OK) return st;
     // the views in up to kChunks contiguous chunks: chunk c's results are
-    // copied back on the copy stream while chunk c + 1 is marched
+    // copied back on the copy stream while chunk c + 1 is marched.  Chunks
+    // alternate between s and march_stream (they write disjoint views and
+    // only read the prepared volumes); the focal-spot march shares one
+    // scratch buffer between chunks, so it keeps them all on s.
+    CTFP_CUDA(cudaEventRecord(p->prepared, s));
+    // on every return, nothing of this call is left running on the plan's own
+    // streams (an error part-way must not leave copies into the caller's
+    // host buffers in flight)
+    struct Drain {
+        ctfp_plan* p;
+        ~Drain()
+        {
+            cudaStreamSynchronize(p->march_stream);
+            cudaStreamSynchronize(p->copy_stream);
+        }
+    } drain{p};
+    const bool two = !p->gp.fspot;
+    if (two) CTFP_CUDA(cudaStreamWaitEvent(p->march_stream, p->prepared, 0));
+    // The last chunk's copy is the one the march cannot hide, so it is made a
+    // quarter of the others: P - n_last views in kChunks - 1 chunks, then n_last.
     const int64_t P = p->geom.projNum, npix = p->geom.dNumU * p->geom.dNumV;
-    const int64_t per = (P + kChunks - 1) / kChunks;
+    const int64_t n_last = P >= 2 * kChunks ? std::max<int64_t>(1, (P + kChunks - 1) / kChunks / 4) : 0;
+    const int64_t per = (P - n_last + kChunks - 2) / (kChunks - 1);
     int c = 0;
-    for (int64_t v0 = 0; v0 < P; v0 += per, c++) {
-        const int64_t n = std::min(per, P - v0);
-        st = forward_range(p, dv, v0, n, false, p->d2h_I, p->d2h_IAbs, nullptr, nullptr, stream, false);
+    for (int64_t v0 = 0; v0 < P; c++) {
+        const int64_t n = v0 + per <= P - n_last ? per : (v0 < P - n_last ? P - n_last - v0 : P - v0);
+        const int64_t v_start = v0;
+        v0 += n;
+        cudaStream_t cs = (two && (c & 1)) ? p->march_stream : s;
+        st = forward_range(p, dv, v_start, n, false, p->d2h_I, p->d2h_IAbs, nullptr, nullptr, cs, false);
         if (st != CTFP_OK) return st;
-        CTFP_CUDA(cudaEventRecord(p->chunk_done[c], s));
+        CTFP_CUDA(cudaEventRecord(p->chunk_done[c], cs));
         CTFP_CUDA(cudaStreamWaitEvent(p->copy_stream, p->chunk_done[c], 0));
-        const size_t off = (size_t)(v0 * npix), bytes = (size_t)(n * npix) * sizeof(float);
+        const size_t off = (size_t)(v_start * npix), bytes = (size_t)(n * npix) * sizeof(float);
         CTFP_CUDA(cudaMemcpyAsync(host_I + off, p->d2h_I + off, bytes, cudaMemcpyDeviceToHost, p->copy_stream));
         CTFP_CUDA(cudaMemcpyAsync(host_IAbsorb + off, p->d2h_IAbs + off, bytes, cudaMemcpyDeviceToHost,
                                   p->copy_stream));

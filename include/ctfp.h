@@ -199,8 +199,10 @@ ctfp_status ctfp_forward(ctfp_plan* plan, const float* const* volumes, float* I,
  * up to 16 chunks of views and copies each chunk's I, IAbsorb (host
  * [projNum][dNumV][dNumU]) back on a plan-owned stream while the next chunk is
  * marched, then I0 (host [dNumV][dNumU], may be NULL), and synchronises the
- * stream.  Page-locked host buffers make the copies asynchronous DMA (and let
- * them overlap the march). */
+ * stream.  The chunks alternate between the given stream and a second
+ * plan-owned stream, so one chunk's last wave overlaps the next chunk's first
+ * (with a focal spot set they all run on the given stream).  Page-locked host
+ * buffers make the copies asynchronous DMA (and let them overlap the march). */
 ctfp_status ctfp_forward_host(ctfp_plan* plan, const float* const* host_volumes, float* host_I,
                               float* host_IAbsorb, float* host_I0, void* stream);
 
