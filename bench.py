@@ -431,7 +431,6 @@ def main():
         L = torch.empty((n_local, V, U, M), device=dev)
         T = pr.forward([v * 0.97 for v in vols], views=vr)["I"]
         logT = torch.log(T)
-        del T
         grads = [torch.zeros_like(v) for v in vols]
         loss = torch.zeros((), device=dev)
         sp = None
@@ -461,7 +460,9 @@ def main():
         fa_ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
         fa = {"value": total_rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms,
               "loss": "sum (log I - log T)^2, T = projection of the phantom x 0.97", "last_loss": float(loss)}
-        del L, logT
+        fa["fused"] = None if sharded else fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays,
+                                                             fa_ms, ws, stream)
+        del L, logT, T
 
     # ---------------- uneven batch: batched vs loop of plain calls ----------
     batch = None
@@ -511,6 +512,52 @@ def main():
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays, fa_ms, ws, stream):
+    """The same forward + loss + adjoint step as one persistent kernel
+    (ctfp_batch_forward_adjoint on a one-item batch: no L checkpoint, no
+    separate dLoss/dI and backward launches), timed like the unfused step; then
+    one step of each into zeroed gradients to compare them."""
+    import torch
+
+    from ct_forward_projection_b200._capi import CtfpError
+    from ct_forward_projection_b200.projector import Batch
+    try:
+        b1 = Batch([pr])
+    except CtfpError as e:
+        return {"unsupported": str(e)}
+    g_f = [torch.zeros_like(v) for v in vols]
+    loss_f = torch.zeros(1, device=vols[0].device)
+    I_f = torch.empty_like(T)
+
+    def step():
+        loss_f.zero_()
+        b1.forward_adjoint([vols], [T], grads=[g_f], I_out=[I_f], loss=loss_f)
+
+    for _ in range(2):
+        step()
+    barrier_sync(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_fa):
+        step()
+    e1.record(stream)
+    barrier_sync(ws)
+    ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
+    for x in g_f + grads:
+        x.zero_()
+    step()
+    fa_step()
+    torch.cuda.synchronize()
+    gdiff = max(float(torch.max(torch.abs(a - c)) / torch.max(torch.abs(c)).clamp_min(1e-30))
+                for a, c in zip(g_f, grads))
+    ldiff = abs(float(loss_f[0]) - float(loss)) / max(abs(float(loss)), 1e-30)
+    b1.close()
+    return {"value": total_rays / (ms / 1e3), "unit": "rays/s", "ms_per_step": ms, "speedup_vs_unfused": fa_ms / ms,
+            "max_rel_diff_grad_vs_unfused": gdiff, "rel_diff_loss_vs_unfused": ldiff,
+            "note": "ctfp_batch_forward_adjoint on a one-item batch: forward, loss and adjoint in one "
+                    "persistent kernel replayed as a CUDA graph, then the fold"}
 
 
 def batch_leg(args, ws, rank, local, stream):

@@ -154,6 +154,42 @@ def test_autograd_binding(cuda_ok):
     assert abs(an - fd) / abs(fd) < 1e-2
 
 
+def test_fused_log_loss_binding(cuda_ok):
+    # LogIntensityLoss (the fused forward + loss + adjoint kernel) gives the
+    # loss and gradients of sum (log I - log T)^2 computed through project(),
+    # scales its gradient by the incoming one, and replays its graph on a
+    # second call; hardware-texture plans are refused
+    from ct_forward_projection_b200._capi import CtfpError
+    from ct_forward_projection_b200.autograd import LogIntensityLoss, project
+    d = small_geometry(n=(13, 12, 10), views=4, U=14, V=10)
+    M = 2
+    vols = random_volumes(d, M, 72)
+    S, mu, G, D = spectral_setup(d, M, 7, 9)
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    target = O.forward(d, [v * np.float32(0.95) for v in vols], mu, W)["I"]
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        T = torch.from_numpy(target.astype(np.float32)).cuda().view(pr.shape_proj)
+        xs = [torch.from_numpy(v).cuda().requires_grad_(True) for v in vols]
+        I, _, _ = project(pr, *xs)
+        ref = torch.sum((torch.log(I) - torch.log(T)) ** 2)
+        ref.backward()
+        with LogIntensityLoss(pr) as lf:
+            for _ in range(2):
+                ys = [torch.from_numpy(v).cuda().requires_grad_(True) for v in vols]
+                loss = lf(T, *ys)
+                (2.0 * loss).backward()
+                torch.cuda.synchronize()
+                assert abs(float(loss.detach()) - float(ref.detach())) <= 1e-5 * abs(float(ref.detach()))
+                for m in range(M):
+                    err = torch.max(torch.abs(ys[m].grad - 2.0 * xs[m].grad)) / torch.max(torch.abs(2.0 * xs[m].grad))
+                    assert float(err) < 1e-5
+    with Projector(d, M, "texture") as pt:
+        pt.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        with pytest.raises(CtfpError):
+            LogIntensityLoss(pt)
+
+
 def test_view_ranges_compose_the_full_projection(cuda_ok):
     # ctfp_forward_views / ctfp_backward_views on three contiguous ranges (what
     # three GPUs of a view-sharded projection run) give the full forward
