@@ -125,7 +125,7 @@ __device__ __forceinline__ void batch_scatter(const ItemDesc& it, const RaySeg& 
     ScatterRun<M> run;
     for (int i = s.i0; i < s.i1; i++)
         run.template add<MODE>(it.gexp, it.g.nx, it.g.ny, it.g.nz, batch_corner<MODE>(it, s, r, i), g);
-    run.flush(it.gexp, it.g.nx, it.g.ny, it.g.nz);
+    run.flush(it.gexp, it.g.nx, it.g.ny, it.g.nz, g);
 }
 
 // One ray.  ADJOINT: the fused forward + loss + adjoint; returns the ray's

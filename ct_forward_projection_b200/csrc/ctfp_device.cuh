@@ -386,15 +386,17 @@ __device__ __forceinline__ void red_add_v4(float4* p, float a, float b, float c,
                  : "memory");
 }
 
-// Adjoint contributions of consecutive samples that share a footprint, summed
-// in registers and sent with one pair of vector reductions per material when
-// the footprint changes (and at the end of the ray): the same sums as one
-// reduction pair per sample, in fewer L2 atomics.
+// Adjoint contributions of consecutive samples that share a footprint.  A
+// ray's dLoss/dL_m (g[m]) is the same at every sample, so a run needs only
+// the sum of its samples' 8 weights; at the footprint's end (and at the end of
+// the ray) each material receives g[m] times that sum as one pair of vector
+// reductions: the same sums as one reduction pair per sample, in fewer L2
+// atomics, with 8 accumulators whatever the material count.
 template <int M>
 struct ScatterRun {
     int ix = INT_MIN, iy = 0, iz = 0;
-    float a[M][8];
-    __device__ __forceinline__ void flush(float4* const* __restrict__ gexp, int nx, int ny, int nz)
+    float a[8];
+    __device__ __forceinline__ void flush(float4* const* __restrict__ gexp, int nx, int ny, int nz, const float* g)
     {
         if (ix == INT_MIN) return;
         if (ix < -1 || iy < -1 || iz < -1 || ix >= nx || iy >= ny || iz >= nz) return;
@@ -402,8 +404,8 @@ struct ScatterRun {
         const size_t i1 = exp_index(nx, ny, ix, iy, iz + 1);
 #pragma unroll
         for (int m = 0; m < M; m++) {
-            red_add_v4(gexp[m] + i0, a[m][0], a[m][1], a[m][2], a[m][3]);
-            red_add_v4(gexp[m] + i1, a[m][4], a[m][5], a[m][6], a[m][7]);
+            red_add_v4(gexp[m] + i0, a[0] * g[m], a[1] * g[m], a[2] * g[m], a[3] * g[m]);
+            red_add_v4(gexp[m] + i1, a[4] * g[m], a[5] * g[m], a[6] * g[m], a[7] * g[m]);
         }
     }
     template <int MODE>
@@ -419,17 +421,13 @@ struct ScatterRun {
             w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
         }
         if (c.ix != ix || c.iy != iy || c.iz != iz) {
-            flush(gexp, nx, ny, nz);
+            flush(gexp, nx, ny, nz, g);
             ix = c.ix; iy = c.iy; iz = c.iz;
 #pragma unroll
-            for (int m = 0; m < M; m++)
-#pragma unroll
-                for (int k = 0; k < 8; k++) a[m][k] = w[k] * g[m];
+            for (int k = 0; k < 8; k++) a[k] = w[k];
         } else {
 #pragma unroll
-            for (int m = 0; m < M; m++)
-#pragma unroll
-                for (int k = 0; k < 8; k++) a[m][k] = fmaf(w[k], g[m], a[m][k]);
+            for (int k = 0; k < 8; k++) a[k] += w[k];
         }
     }
 };

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
                 run.template add<INTERP_TEXEMU>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz,
                                                 corner_tex(ref32_coords(prm.g, r, i)), g);
         }
-        run.flush(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz);
+        run.flush(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, g);
     }
 }
 
