@@ -194,15 +194,13 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
 // caps: 65536 / (64 * minb)); the fused adjoint carries the scatter's run
 // accumulators on top of the march, and the texture emulation's FP32
 // reference coordinates take more registers than the FP64 trilinear ones.
-// For the trilinear fused adjoint, 12 CTAs (M <= 2) measured 2 % faster than
-// 10 or 14 on a 12-problem batch, and 8 slower.  The texture-emulation caps
-// are the tightest without spills; the trilinear kernels for 3 and 4
-// materials keep 4-20 bytes of spill stores at every cap tried (88-128
-// registers), so theirs follow the measured batch.
+// For the trilinear fused adjoint, 12 CTAs (M <= 2) measured as fast as 14
+// or 16 and 2 % faster than 10 on a 12-problem batch; 8 was slower.  Every
+// cap leaves its kernel without spills (ptxas -v).
 template <bool ADJOINT, int M, int MODE>
 struct BatchBudget {
     static constexpr int minb = MODE == INTERP_TRILINEAR
-                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : (M <= 2 ? 16 : 12))
+                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : (M <= 2 ? 16 : 10))
                                     : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 12 : 10));
 };
 
