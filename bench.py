@@ -279,30 +279,34 @@ def main():
     from ct_forward_projection_b200 import physics
     from ct_forward_projection_b200.projector import Projector
 
-    ws, rank, local = dist_setup(args.gpus)
-    w = physics.workload(args.workload)
-    sharded = args.shard == "views" and ws > 1
-    if not sharded:
-        w.seed += rank  # each rank projects its own object
-    dev = f"cuda:{local}"
-
     if args.impl == "reference":
+        # rank 0 alone runs the reference's implementation; under torchrun the
+        # other ranks exit at once, and no process group is formed, so nothing
+        # waits on a rank that has left
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        if rank != 0:
+            return
+        torch.cuda.set_device(local)
+        w = physics.workload(args.workload)
         w._vols = physics.phantom(w, "cpu")
-        from oracle import oracle as O
-        pr_tmp = None
         # energy weights for the oracle, built through the library's table builders
         pr_tmp = Projector(w.geometry, len(w.materials), "trilinear", local)
         pr_tmp.set_tables_from_workload(w)
         w._W = _weights_from_tables(w, local)
         pr_tmp.close()
         line = reference_arm(args, w, ws, rank)
-        if rank == 0 and line is not None:
+        if line is not None:
             print(json.dumps(line), flush=True)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-            dist.destroy_process_group()
         return
+
+    ws, rank, local = dist_setup(args.gpus)
+    w = physics.workload(args.workload)
+    sharded = args.shard == "views" and ws > 1
+    if not sharded:
+        w.seed += rank  # each rank projects its own object
+    dev = f"cuda:{local}"
 
     vols = physics.phantom(w, dev)
     M = len(vols)

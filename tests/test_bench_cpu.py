@@ -50,3 +50,14 @@ def test_clock_sampler_without_a_window_keeps_every_sample(tmp_path, monkeypatch
     r = c.stop()
     assert r["window"].startswith("whole run")
     assert r["samples"] >= 1 and r["sm_mhz"] == 1500.0 and r["reasons"] == []
+
+
+def test_reference_arm_other_ranks_exit_at_once():
+    # under torchrun only rank 0 runs the reference arm; the others leave with
+    # status 0 and print nothing, before any process group or GPU work
+    import subprocess
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT="29591")
+    r = subprocess.run([sys.executable, os.path.join(os.path.dirname(bench.__file__), "bench.py"), "--impl",
+                        "reference", "--gpus", "2"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
