@@ -81,6 +81,34 @@ def test_forward_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
     assert rel_err_scaled(out["L"].cpu().numpy().reshape(-1, M), ref["L"]) < RTOL_TRI
 
 
+# voxels of different size on each axis (1.0 x 0.75 x 2.5 mm): the reference
+# divides each texture coordinate by its own axis's voxel size
+# (CBCTPolyProjGPU.cu:1915-1920) while the ray step is half the x voxel
+ANISO = dict(pNumX=20, pNumY=16, pNumZ=10, pLengthX=20.0, pLengthY=12.0, pLengthZ=25.0, projNum=5, dNumU=24,
+             dNumV=16, dSize=2.0, sod=300.0, sdd=450.0, rotatedDirection=1)
+
+
+@pytest.mark.parametrize("mode,sampler", [("trilinear", "layered"), ("trilinear", "global"), ("trilinear", "brick"),
+                                          ("texemu", "layered"), ("texture", None)])
+def test_anisotropic_voxels_vs_oracle(cuda_ok, mode, sampler):
+    d = dict(ANISO)
+    M = 2
+    vols = random_volumes(d, M, 404)
+    S, mu, G, D = spectral_setup(d, M, 9, 41)
+    W = O.energy_weights(d, S, G, 2, D, 60000.0)
+    ref = O.forward(d, vols, mu, W, O.TRILINEAR if mode == "trilinear" else O.TEXEMU)
+    with Projector(d, M, mode) as pr:
+        if sampler:
+            pr.set_sampler(sampler)
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        out = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    tol = RTOL_TRI if mode == "trilinear" else RTOL_TEX
+    assert rel_err(out["I"].cpu(), ref["I"]) < tol
+    assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < tol
+    assert rel_err_scaled(out["L"].cpu().numpy().reshape(-1, M), ref["L"]) < (RTOL_TRI if mode == "trilinear" else 1e-3)
+
+
 @pytest.mark.parametrize("layout", [0, 1, 2])
 def test_forward_grid_layouts_and_no_response(cuda_ok, layout):
     d = small_geometry(n=16, views=4, U=24, V=10)
