@@ -120,7 +120,7 @@ ctfp_status check_geometry(const ctfp_geometry* g)
     if (!(g->pLengthX > 0.f && g->pLengthY > 0.f && g->pLengthZ > 0.f))
         return fail(CTFP_INVALID_ARG, "pLengthX/pLengthY/pLengthZ must be positive");
     if (g->projNum <= 0 || g->projNum > 1000000) return fail(CTFP_INVALID_ARG, "projNum out of range");
-    if (g->dNumU <= 0 || g->dNumV <= 0 || g->dNumU > 65536 || g->dNumV > 65536)
+    if (g->dNumU <= 0 || g->dNumV <= 0 || g->dNumU > 65535 || g->dNumV > 65535)
         return fail(CTFP_INVALID_ARG, "dNumU/dNumV out of range");
     if (!(g->dSize > 0.f)) return fail(CTFP_INVALID_ARG, "dSize must be positive");
     if (!(g->sod > 0.f) || !(g->sdd > g->sod)) return fail(CTFP_INVALID_ARG, "need 0 < sod < sdd");

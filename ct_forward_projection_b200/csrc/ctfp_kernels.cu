@@ -604,11 +604,12 @@ dim3 march_grid(const MarchParams& prm, const LaunchShape& ls)
 
 }  // namespace
 
-cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sampler, bool do_spectral,
-                           const LaunchShape& ls, cudaStream_t st)
+namespace {
+
+// One launch over prm.n_views views (at most 65535 view groups: grid.z).
+cudaError_t launch_forward_once(const MarchParams& prm, int M, int interp, int sampler, bool do_spectral,
+                                const LaunchShape& ls, cudaStream_t st)
 {
-    MarchParams prm = prm_in;
-    prm.views_per_cta = ls.views_per_cta;
     if (sampler == SAMPLER_BRICK && interp != INTERP_TEXTURE) {
         const dim3 grid((prm.g.U + kBU - 1) / kBU, (prm.g.V + kBV - 1) / kBV,
                         (prm.n_views + ls.views_per_cta - 1) / ls.views_per_cta);
@@ -632,6 +633,25 @@ cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sam
         case 4: return fwd_dispatch_mode<4>(prm, interp, sampler, do_spectral, ls.min_ctas, grid, block, smem, st);
     }
     return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sampler, bool do_spectral,
+                           const LaunchShape& ls, cudaStream_t st)
+{
+    // view groups run along grid.z, at most 65535 per launch
+    const int vpc = ls.views_per_cta;
+    const int max_views = 65535 * vpc;
+    for (int v0 = 0; v0 < prm_in.n_views; v0 += max_views) {
+        MarchParams prm = prm_in;
+        prm.views_per_cta = vpc;
+        prm.view0 = prm_in.view0 + v0;
+        prm.n_views = std::min(max_views, prm_in.n_views - v0);
+        const cudaError_t e = launch_forward_once(prm, M, interp, sampler, do_spectral, ls, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st)

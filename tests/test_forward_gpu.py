@@ -259,6 +259,30 @@ def test_degenerate_detectors(cuda_ok, U, V, P):
     assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
 
 
+def test_more_views_than_one_launch_holds(cuda_ok):
+    # 70000 views at one view per CTA exceed the 65535 CTAs of grid.z: the
+    # forward and the adjoint launch in view chunks and still equal the oracle
+    d = small_geometry(n=4, views=70000, U=2, V=2, length=4.0)
+    M = 1
+    vols = random_volumes(d, M, 90)
+    S, mu, G, D = spectral_setup(d, M, 3, 91)
+    W = O.energy_weights(d, S, G, 2, D, 60000.0)
+    ref = O.forward(d, vols, mu, W, O.TRILINEAR)
+    rng = np.random.RandomState(4)
+    gL = rng.normal(size=(d["projNum"] * 4, M)).astype(np.float32)
+    gref = O.line_integrals_adjoint(d, gL, M, O.TRILINEAR)
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_launch_shape(32, 1, 1, 2)
+        pr.set_spectral_tables(S, mu, G, 2, D, 60000.0)
+        out = pr.forward(to_dev(vols), want_L=True)
+        g = pr.line_integrals_adjoint(torch.from_numpy(gL.reshape(d["projNum"], 2, 2, M)).cuda())
+        torch.cuda.synchronize()
+    assert rel_err(out["I"].cpu(), ref["I"]) < RTOL_TRI
+    assert rel_err_scaled(out["L"].cpu().numpy().reshape(-1, M), ref["L"]) < RTOL_TRI
+    a = g[0].double().cpu().numpy()
+    assert np.max(np.abs(a - gref[0])) / np.max(np.abs(gref[0])) < 1e-5
+
+
 def test_rays_missing_volume_are_zero(cuda_ok):
     # a detector offset so far that every ray passes beside the volume
     d = small_geometry(n=8, views=2, U=6, V=6, length=8.0, pitch=60.0)
