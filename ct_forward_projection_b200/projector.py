@@ -52,6 +52,33 @@ def _dptr(t) -> int | None:
     return t.data_ptr()
 
 
+def _dp(t, numel: int, name: str, device: int) -> int | None:
+    """Device pointer of an argument after the checks the C ABI cannot make
+    (it sees only the pointer): a contiguous float32 tensor on the plan's
+    device with exactly the number of elements the call reads or writes."""
+    if t is None:
+        return None
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+        raise TypeError(f"{name}: a contiguous float32 CUDA tensor is required")
+    if t.device.index != device:
+        raise ValueError(f"{name} is on {t.device}; the plan is on cuda:{device}")
+    if t.numel() != numel:
+        raise ValueError(f"{name} holds {t.numel()} elements; the call needs {numel}")
+    return t.data_ptr()
+
+
+def _hp(a, numel: int, name: str):
+    """Host pointer of an argument (numpy array or CPU tensor, float32,
+    contiguous) holding exactly numel elements."""
+    if a is None:
+        return None
+    n = a.size if isinstance(a, np.ndarray) else a.numel()
+    if n != numel:
+        raise ValueError(f"{name} holds {n} elements; the call needs {numel}")
+    return _host_ptr(a)
+
+
 def _stream(stream) -> int | None:
     import torch
     if stream is None:
@@ -182,11 +209,18 @@ class Projector:
         self.set_spectral_tables(w.spectrum(), w.mu_table(), G, layout if G is not None else 0, D, w.I0Val)
 
     # -- compute ------------------------------------------------------------
-    def _vol_ptrs(self, volumes: Sequence):
-        assert len(volumes) == self.M, f"expected {self.M} volumes"
+    @property
+    def n_voxels(self) -> int:
+        z, y, x = self.shape_vol
+        return z * y * x
+
+    def _vol_ptrs(self, volumes: Sequence, name: str = "volume"):
+        if len(volumes) != self.M:
+            raise ValueError(f"expected {self.M} {name}s, got {len(volumes)}")
         for v in volumes:
-            assert tuple(v.shape) == self.shape_vol, f"volume shape {tuple(v.shape)} != {self.shape_vol}"
-        return ptr_array([_dptr(v) for v in volumes])
+            if tuple(v.shape) != self.shape_vol:
+                raise ValueError(f"{name} shape {tuple(v.shape)} != {self.shape_vol}")
+        return ptr_array([_dp(v, self.n_voxels, name, self.device) for v in volumes])
 
     def forward(self, volumes: Sequence, want_L: bool = False, out=None, stream=None, views=None) -> dict:
         """Fused march + spectral epilogue. Returns dict(I, IAbsorb, I0[, L]).
@@ -201,12 +235,13 @@ class Projector:
                    "I0": torch.empty((V, U), device=dev)}
             if want_L:
                 out["L"] = torch.empty((n, V, U, self.M), device=dev)
+        d = self.device
+        ptrs = (_dp(out.get("I"), n * V * U, "I", d), _dp(out.get("IAbsorb"), n * V * U, "IAbsorb", d),
+                _dp(out.get("I0"), V * U, "I0", d), _dp(out.get("L"), n * V * U * self.M, "L", d))
         if views is None:
-            call("ctfp_forward", self._h, self._vol_ptrs(volumes), _dptr(out.get("I")), _dptr(out.get("IAbsorb")),
-                 _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
+            call("ctfp_forward", self._h, self._vol_ptrs(volumes), *ptrs, _stream(stream))
         else:
-            call("ctfp_forward_views", self._h, self._vol_ptrs(volumes), int(views[0]), n, _dptr(out.get("I")),
-                 _dptr(out.get("IAbsorb")), _dptr(out.get("I0")), _dptr(out.get("L")), _stream(stream))
+            call("ctfp_forward_views", self._h, self._vol_ptrs(volumes), int(views[0]), n, *ptrs, _stream(stream))
         return out
 
     def forward_host(self, host_volumes: Sequence[np.ndarray], out: dict | None = None) -> dict:
@@ -215,9 +250,11 @@ class Projector:
         if out is None:
             out = {"I": np.empty((P, V, U), np.float32), "IAbsorb": np.empty((P, V, U), np.float32),
                    "I0": np.empty((V, U), np.float32)}
-        ptrs = ptr_array([_host_ptr(v) for v in host_volumes])
-        call("ctfp_forward_host", self._h, ptrs, _host_ptr(out["I"]), _host_ptr(out["IAbsorb"]),
-             _host_ptr(out.get("I0")), _stream(None))
+        if len(host_volumes) != self.M:
+            raise ValueError(f"expected {self.M} volumes, got {len(host_volumes)}")
+        ptrs = ptr_array([_hp(v, self.n_voxels, "volume") for v in host_volumes])
+        call("ctfp_forward_host", self._h, ptrs, _hp(out["I"], P * V * U, "I"),
+             _hp(out["IAbsorb"], P * V * U, "IAbsorb"), _hp(out.get("I0"), V * U, "I0"), _stream(None))
         return out
 
     def line_integrals(self, volumes: Sequence, out=None, stream=None):
@@ -225,7 +262,8 @@ class Projector:
         P, V, U = self.shape_proj
         if out is None:
             out = torch.empty((P, V, U, self.M), device=f"cuda:{self.device}")
-        call("ctfp_line_integrals", self._h, self._vol_ptrs(volumes), _dptr(out), _stream(stream))
+        call("ctfp_line_integrals", self._h, self._vol_ptrs(volumes), _dp(out, P * V * U * self.M, "L", self.device),
+             _stream(stream))
         return out
 
     def spectral_from_L(self, L, stream=None) -> dict:
@@ -233,7 +271,8 @@ class Projector:
         P, V, U = self.shape_proj
         dev = f"cuda:{self.device}"
         out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
-        call("ctfp_spectral_from_L", self._h, _dptr(L), _dptr(out["I"]), _dptr(out["IAbsorb"]), _stream(stream))
+        call("ctfp_spectral_from_L", self._h, _dp(L, P * V * U * self.M, "L", self.device), _dptr(out["I"]),
+             _dptr(out["IAbsorb"]), _stream(stream))
         return out
 
     def backward(self, L, gI=None, gIAbsorb=None, grads=None, stream=None, views=None) -> list:
@@ -243,20 +282,25 @@ class Projector:
         import torch
         if grads is None:
             grads = [torch.zeros(self.shape_vol, device=f"cuda:{self.device}") for _ in range(self.M)]
-        gp = ptr_array([_dptr(g) for g in grads])
+        P, V, U = self.shape_proj
+        n = P if views is None else int(views[1])
+        d = self.device
+        gp = self._vol_ptrs(grads, "gradient")
+        args = (_dp(L, n * V * U * self.M, "L", d), _dp(gI, n * V * U, "gI", d),
+                _dp(gIAbsorb, n * V * U, "gIAbsorb", d))
         if views is None:
-            call("ctfp_backward", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), gp, _stream(stream))
+            call("ctfp_backward", self._h, *args, gp, _stream(stream))
         else:
-            call("ctfp_backward_views", self._h, _dptr(L), _dptr(gI), _dptr(gIAbsorb), int(views[0]), int(views[1]),
-                 gp, _stream(stream))
+            call("ctfp_backward_views", self._h, *args, int(views[0]), n, gp, _stream(stream))
         return grads
 
     def line_integrals_adjoint(self, gL, grads=None, stream=None) -> list:
         import torch
         if grads is None:
             grads = [torch.zeros(self.shape_vol, device=f"cuda:{self.device}") for _ in range(self.M)]
-        call("ctfp_line_integrals_adjoint", self._h, _dptr(gL), ptr_array([_dptr(g) for g in grads]),
-             _stream(stream))
+        P, V, U = self.shape_proj
+        call("ctfp_line_integrals_adjoint", self._h, _dp(gL, P * V * U * self.M, "gL", self.device),
+             self._vol_ptrs(grads, "gradient"), _stream(stream))
         return grads
 
     def count_support_samples(self) -> int:
@@ -293,11 +337,22 @@ class Batch:
         call("ctfp_batch_info", self._h, C.byref(u), C.byref(g0), C.byref(g1))
         return {"units": int(u.value), "grid_forward": int(g0.value), "grid_adjoint": int(g1.value)}
 
-    def _vol_table(self, volumes):
-        assert len(volumes) == len(self.projectors)
-        per = [p._vol_ptrs(v) for p, v in zip(self.projectors, volumes)]
-        self._keep = per
+    def _vol_table(self, volumes, name: str = "volume"):
+        if len(volumes) != len(self.projectors):
+            raise ValueError(f"expected {len(self.projectors)} items, got {len(volumes)}")
+        per = [p._vol_ptrs(v, name) for p, v in zip(self.projectors, volumes)]
+        self._keep = self._keep + per
         return ptr_array([C.cast(a, C.c_void_p).value for a in per])
+
+    def _item_ptrs(self, tensors, per_ray: int, name: str):
+        """One pointer per item: tensors[k] holds rays(k) * per_ray floats."""
+        if len(tensors) != len(self.projectors):
+            raise ValueError(f"expected {len(self.projectors)} {name} entries, got {len(tensors)}")
+        out = []
+        for p, t in zip(self.projectors, tensors):
+            P, V, U = p.shape_proj
+            out.append(_dp(t, P * V * U * (p.M if per_ray < 0 else per_ray), name, p.device))
+        return ptr_array(out)
 
     def _out(self, want_L: bool = False) -> list:
         import torch
@@ -314,10 +369,11 @@ class Batch:
     def forward(self, volumes: Sequence[Sequence], want_L: bool = False, out: list | None = None, stream=None) -> list:
         """volumes[k] = the M density maps of item k; returns [dict(I, IAbsorb[, L])]."""
         out = out if out is not None else self._out(want_L)
+        self._keep = []
         vt = self._vol_table(volumes)
-        I = ptr_array([_dptr(o["I"]) for o in out])
-        A = ptr_array([_dptr(o.get("IAbsorb")) for o in out])
-        L = ptr_array([_dptr(o.get("L")) for o in out]) if any("L" in o for o in out) else None
+        I = self._item_ptrs([o["I"] for o in out], 1, "I")
+        A = self._item_ptrs([o.get("IAbsorb") for o in out], 1, "IAbsorb")
+        L = self._item_ptrs([o.get("L") for o in out], -1, "L") if any("L" in o for o in out) else None
         call("ctfp_batch_forward", self._h, vt, I, A, L, _stream(stream))
         return out
 
@@ -330,13 +386,13 @@ class Batch:
                      for p in self.projectors]
         if loss is None:
             loss = torch.zeros(len(self.projectors), device=f"cuda:{self.projectors[0].device}")
+        self._keep = []
         vt = self._vol_table(volumes)
-        gtabs = [ptr_array([_dptr(g) for g in gk]) for gk in grads]
-        self._keep = self._keep + gtabs
-        G = ptr_array([C.cast(a, C.c_void_p).value for a in gtabs])
-        T = ptr_array([_dptr(t) for t in targets])
-        I = ptr_array([_dptr(t) for t in I_out]) if I_out is not None else None
-        call("ctfp_batch_forward_adjoint", self._h, vt, T, I, G, _dptr(loss), _stream(stream))
+        G = self._vol_table(grads, "gradient")
+        T = self._item_ptrs(targets, 1, "target")
+        I = self._item_ptrs(I_out, 1, "I") if I_out is not None else None
+        lp = _dp(loss, len(self.projectors), "loss", self.projectors[0].device) if loss is not None else None
+        call("ctfp_batch_forward_adjoint", self._h, vt, T, I, G, lp, _stream(stream))
         return {"grads": grads, "loss": loss, "I": I_out}
 
 

@@ -283,6 +283,43 @@ def test_more_views_than_one_launch_holds(cuda_ok):
     assert np.max(np.abs(a - gref[0])) / np.max(np.abs(gref[0])) < 1e-5
 
 
+def test_host_mirror_rejects_wrong_buffers(cuda_ok):
+    # the C ABI sees only pointers; the Python mirror checks every buffer's
+    # element count, dtype and device before a call, so a wrong buffer is an
+    # exception on the host and never an out-of-bounds access on the GPU
+    from ct_forward_projection_b200 import Batch
+    d = small_geometry(n=8, views=3, U=10, V=6)
+    M = 2
+    vols = to_dev(random_volumes(d, M, 11))
+    S, mu, G, D = spectral_setup(d, M, 4, 12)
+    with Projector(d, M, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        good = pr.forward(vols, want_L=True)
+        bad_I = {**good, "I": torch.empty(3 * 6 * 10 - 1, device="cuda")}
+        with pytest.raises(ValueError):
+            pr.forward(vols, out=bad_I)
+        with pytest.raises(ValueError):
+            pr.forward(vols[:1])
+        with pytest.raises(TypeError):
+            pr.forward([v.double() for v in vols])
+        with pytest.raises(ValueError):
+            pr.forward(vols, out={**good, "L": torch.empty(3, 6, 10, 1, device="cuda")})
+        with pytest.raises(ValueError):
+            pr.backward(good["L"], gI=torch.ones(3, 6, 9, device="cuda"))
+        with pytest.raises(ValueError):
+            pr.backward(good["L"], gI=torch.ones_like(good["I"]), grads=[torch.zeros(8, 8, 7, device="cuda")] * M)
+        with pytest.raises(ValueError):
+            pr.forward_host([v.cpu().numpy() for v in vols], out={"I": np.empty(5, np.float32),
+                                                                   "IAbsorb": np.empty((3, 6, 10), np.float32)})
+        b = Batch([pr])
+        with pytest.raises(ValueError):
+            b.forward_adjoint([vols], [torch.ones(3, 6, 11, device="cuda")])
+        out = b.forward_adjoint([vols], [good["I"] * 0.9])
+        torch.cuda.synchronize()
+        assert torch.isfinite(out["loss"]).all()
+        b.close()
+
+
 def test_rays_missing_volume_are_zero(cuda_ok):
     # a detector offset so far that every ray passes beside the volume
     d = small_geometry(n=8, views=2, U=6, V=6, length=8.0, pitch=60.0)
