@@ -69,6 +69,7 @@ _SIGNATURES = {
     "ctfp_plan_set_interp": (C.c_int, [_P, C.c_int32]),
     "ctfp_plan_set_sampler": (C.c_int, [_P, C.c_int32]),
     "ctfp_plan_set_skip_empty": (C.c_int, [_P, C.c_int32]),
+    "ctfp_plan_check_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "ctfp_plan_set_focal_spot": (C.c_int, [_P, _P, _P]),
     "ctfp_focal_spot_offsets": (C.c_int, [C.c_int64, C.c_float, _P, _P]),
     "ctfp_plan_set_launch_shape": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),

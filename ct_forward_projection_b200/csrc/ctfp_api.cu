@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -46,6 +47,8 @@ struct ctfp_plan {
     // volumes at every call
     bool skip_empty = false;
     uint8_t* d_occ = nullptr;
+    // device status word written by kernels whose bounded waits ran out
+    unsigned* d_status = nullptr;
     // focal spot (off unless set): per-view offsets, and the march's raw
     // line integrals before the re-alignment (grown on demand)
     float2* d_fspot = nullptr;
@@ -253,6 +256,16 @@ ctfp_status upload_textures(ctfp_plan* p, const float* const* volumes, cudaStrea
     return CTFP_OK;
 }
 
+// Polls of a TMA completion before a CTA of the TMA-staged brick sampler gives
+// up staging (a completion normally takes a few microseconds; the default
+// bounds the wait near a millisecond).  CTFP_WAIT_LIMIT overrides it.
+int wait_limit()
+{
+    const char* e = std::getenv("CTFP_WAIT_LIMIT");
+    if (e && *e) return std::max(0, std::atoi(e));
+    return 1 << 16;
+}
+
 MarchParams base_params(const ctfp_plan* p)
 {
     MarchParams prm;
@@ -272,6 +285,8 @@ MarchParams base_params(const ctfp_plan* p)
         prm.occ_x = occ_dim(p->gp.nx);
         prm.occ_y = occ_dim(p->gp.ny);
     }
+    prm.status = p->d_status;
+    prm.wait_limit = wait_limit();
     return prm;
 }
 
@@ -343,6 +358,21 @@ extern "C" {
 
 const char* ctfp_last_error_string(void) { return g_last_error.c_str(); }
 
+ctfp_status ctfp_plan_check_status(ctfp_plan* p, uint32_t* flags)
+{
+    if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
+    DeviceScope ds(p->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    CTFP_CUDA(cudaDeviceSynchronize());
+    unsigned v = 0;
+    CTFP_CUDA(cudaMemcpy(&v, p->d_status, sizeof(v), cudaMemcpyDeviceToHost));
+    CTFP_CUDA(cudaMemset(p->d_status, 0, sizeof(v)));
+    if (flags) *flags = v;
+    if (v & kCtfpStatusWaitTimeout)
+        return fail(CTFP_TIMEOUT, "a TMA-staged brick wait ran out; those samples were read from the volume");
+    return CTFP_OK;
+}
+
 const char* ctfp_version(void) { return "ctfp 0.1.0 (sm_100a)"; }
 
 ctfp_status ctfp_compute_paras(const ctfp_geometry* g, ctfp_system_info* out)
@@ -408,6 +438,8 @@ ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_
     if (e == cudaSuccess)
         e = cudaMemcpy(p->d_trigf, trigf.data(), sizeof(float2) * trigf.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_status, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(unsigned));
     if (e != cudaSuccess) {
         ctfp_plan_destroy(p);
         return cuda_fail(e, "plan allocation");
@@ -450,6 +482,7 @@ ctfp_status ctfp_plan_destroy(ctfp_plan* p)
     for (int m = 0; m < kMaxM; m++) cudaFree(p->h2d_vol[m]);
     for (int m = 0; m < kMaxM; m++) cudaFree(p->d_gexp[m]);
     cudaFree(p->d_occ);
+    cudaFree(p->d_status);
     for (cudaEvent_t& e : p->chunk_done)
         if (e) cudaEventDestroy(e);
     if (p->copies_done) cudaEventDestroy(p->copies_done);

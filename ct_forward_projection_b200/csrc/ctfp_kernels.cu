@@ -9,8 +9,13 @@
 // all energies (sum_m mu[e][m] * L_m equals the reference's per-energy
 // mu_E-volume integral because trilinear interpolation is linear in the voxel
 // values), and the energy sum runs on the device in compensated FP32.
+#include <cuda.h>
+
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
 
 #include "ctfp_kernels.cuh"
 
@@ -508,34 +513,288 @@ __global__ void __launch_bounds__(kBU * kBV, MINB) k_forward_brick(const MarchPa
     }
 }
 
-template <int M, int MODE, bool SPEC>
-cudaError_t brick_launch(const MarchParams& prm, dim3 grid, size_t smem, cudaStream_t st)
+// ---------------------------------------------------------------------------
+// Brick sampler with TMA staging: the same boxes, the same fit rule and the
+// same reads as k_forward_brick, but each box is one tensor load per material
+// (cp.async.bulk.tensor.3d, issued by one thread, completion counted on an
+// mbarrier) instead of 128 threads' scalar loads.  The box's x origin is
+// rounded down to a multiple of 4 voxels, because a tiled tensor load must
+// start on a 16-byte boundary in x, so kTX = 16 + 3 + 1 columns are staged;
+// y and z start at the box origin, and voxels outside the volume (negative or
+// past the end) arrive as zeros, the texture border.  The dense box layout is
+// the one TMA writes: rows of kTX floats, slices of kTX * kBY floats.
+//
+// Every wait is bounded: thread 0 issues, all threads poll the mbarrier at
+// most prm.wait_limit times; when any gives up, the CTA reads that segment and
+// all later ones from the volume (same results), ors kCtfpStatusWaitTimeout
+// into the plan's status word, and before exiting waits, again bounded, for
+// the load still in flight so that it cannot land in shared memory the CTA no
+// longer owns.
+constexpr int kTX = 20;
+constexpr int kTRow = kTX, kTSlice = kTX * kBY;
+constexpr int kTBoxFloats = kTSlice * kBZ;  // 6400 floats = 25600 bytes, a multiple of 128
+constexpr int kExitPolls = 1 << 22;
+
+struct BrickMaps {
+    CUtensorMap tm[kMaxM];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
 {
-    // the dynamic shared-memory opt-in is per device; plans on other threads
-    // may get here at the same time (setting the attribute twice is harmless)
-    static std::atomic<unsigned long long> attr_set{0};
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded poll of one mbarrier phase; true when it completed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit)
+{
+    for (int k = 0; k < limit; k++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_box(float* dst, const CUtensorMap* tm, int x, int y, int z, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
+template <int M, int MODE, bool SPECTRAL, int MINB>
+__global__ void __launch_bounds__(kBU * kBV, MINB)
+    k_forward_brick_tma(const MarchParams prm, const __grid_constant__ BrickMaps maps)
+{
+    extern __shared__ unsigned char smem_raw[];
+    float* s_box = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    float* s_mu = s_box + M * kTBoxFloats;  // [E][M]
+    __shared__ int s_red[8];
+    __shared__ __align__(8) uint64_t s_bar;
+    const int tid = threadIdx.y * kBU + threadIdx.x;
+    if (tid == 0) mbar_init(&s_bar, 1);
+    if (SPECTRAL) load_mu(s_mu, prm.mu, prm.E * M);
+    __syncthreads();
+    uint32_t phase = 0;
+    bool staging = true;   // CTA-uniform: false once a wait ran out
+    bool in_flight = false;  // CTA-uniform: a load whose completion was not seen
+    const int u = blockIdx.x * kBU + threadIdx.x;
+    const int v = blockIdx.y * kBV + threadIdx.y;
+    const bool live = u < prm.g.U && v < prm.g.V;
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t pix = (int64_t)v * prm.g.U + u;
+    const int pend = prm.view0 + prm.n_views;
+    constexpr int margin = MODE == INTERP_TRILINEAR ? 0 : 1;
+    for (int k = 0; k < prm.views_per_cta; k++) {
+        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        if (p >= pend) break;
+        RaySeg s;
+        s.i0 = s.i1 = 0;
+        if (live) s = ray_segment(prm.g, p, v, u);
+        RayRef32 r;
+        if (MODE != INTERP_TRILINEAR && live) r = ray_ref32(prm.g, p, v, u);
+        if (tid == 0) {
+            s_red[0] = INT_MAX;
+            s_red[1] = INT_MIN;
+        }
+        __syncthreads();
+        if (s.i1 > s.i0) {
+            atomicMin(&s_red[0], s.i0);
+            atomicMax(&s_red[1], s.i1);
+        }
+        __syncthreads();
+        const int I0 = s_red[0], I1 = s_red[1];
+        __syncthreads();
+        float acc[M], cmp[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+        for (int seg = I0; seg < I1; seg += kBS) {
+            const int a0 = max(seg, s.i0), a1 = min(min(seg + kBS, I1), s.i1);
+            if (tid == 0) {
+                s_red[0] = s_red[1] = s_red[2] = INT_MAX;
+                s_red[3] = s_red[4] = s_red[5] = INT_MIN;
+            }
+            __syncthreads();
+            if (a0 < a1) {
+                const Corner c0 = corner_at<MODE>(prm, s, r, a0), c1 = corner_at<MODE>(prm, s, r, a1 - 1);
+                atomicMin(&s_red[0], min(c0.ix, c1.ix) - margin);
+                atomicMin(&s_red[1], min(c0.iy, c1.iy) - margin);
+                atomicMin(&s_red[2], min(c0.iz, c1.iz) - margin);
+                atomicMax(&s_red[3], max(c0.ix, c1.ix) + margin);
+                atomicMax(&s_red[4], max(c0.iy, c1.iy) + margin);
+                atomicMax(&s_red[5], max(c0.iz, c1.iz) + margin);
+            }
+            __syncthreads();
+            const int ox = s_red[0], oy = s_red[1], oz = s_red[2];
+            bool fits = staging && s_red[3] >= ox && s_red[3] + 1 - ox < kBX && s_red[4] + 1 - oy < kBY &&
+                        s_red[5] + 1 - oz < kBZ;
+            const int ox4 = ox & ~3;  // floor to a multiple of 4: the load starts on a 16-byte boundary
+            if (fits) {
+                if (tid == 0) {
+                    mbar_expect_tx(&s_bar, (uint32_t)(M * kTBoxFloats * sizeof(float)));
+#pragma unroll
+                    for (int m = 0; m < M; m++) tma_load_box(s_box + m * kTBoxFloats, &maps.tm[m], ox4, oy, oz, &s_bar);
+                }
+                const bool done = mbar_wait_bounded(&s_bar, phase, prm.wait_limit);
+                if (__syncthreads_and(done)) {
+                    phase ^= 1u;
+                } else {
+                    // give up staging in this CTA; the load may still land
+                    staging = false;
+                    in_flight = true;
+                    fits = false;
+                    if (tid == 0 && prm.status) atomicOr(prm.status, kCtfpStatusWaitTimeout);
+                }
+            }
+            const int dxa = ox - ox4;
+            for (int i = a0; i < a1; i++) {
+                const Corner c = corner_at<MODE>(prm, s, r, i);
+                const int bx = c.ix - ox, by = c.iy - oy, bz = c.iz - oz;
+                float cv[M][8];
+                if (fits && (unsigned)bx < (unsigned)(kBX - 1) && (unsigned)by < (unsigned)(kBY - 1) &&
+                    (unsigned)bz < (unsigned)(kBZ - 1)) {
+                    const int b = bz * kTSlice + by * kTRow + bx + dxa;
+#pragma unroll
+                    for (int m = 0; m < M; m++) {
+                        const float* q = s_box + m * kTBoxFloats + b;
+                        cv[m][0] = q[0]; cv[m][1] = q[1]; cv[m][2] = q[kTRow]; cv[m][3] = q[kTRow + 1];
+                        cv[m][4] = q[kTSlice]; cv[m][5] = q[kTSlice + 1]; cv[m][6] = q[kTSlice + kTRow];
+                        cv[m][7] = q[kTSlice + kTRow + 1];
+                    }
+                } else {
+                    load8_global<M>(prm.vol, prm.g.nx, prm.g.ny, prm.g.nz, c, cv);
+                }
+#pragma unroll
+                for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], interp8<MODE>(c, cv[m]));
+            }
+            __syncthreads();  // the box is read; the next segment may overwrite it
+        }
+        if (!live) continue;
+        float L[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
+        const int64_t ray = (int64_t)(p - prm.out_view0) * npix + pix;
+        if (prm.L) store_L<M>(prm.L, ray, L);
+        if (SPECTRAL) {
+            float I, A;
+            spectral<M>(s_mu, prm.E, prm.W, pix, npix, L, I, A);
+            if (prm.I) prm.I[ray] = I;
+            if (prm.IAbs) prm.IAbs[ray] = A;
+        }
+    }
+    // a load given up on may still be writing the box: wait for it (bounded)
+    // before the CTA's shared memory is released
+    if (in_flight) mbar_wait_bounded(&s_bar, phase, kExitPolls);
+}
+
+// The dynamic shared-memory opt-in is per device and per kernel; plans on
+// other threads may get here at the same time (setting it twice is harmless).
+template <typename K>
+cudaError_t opt_in_smem(K kernel, std::atomic<unsigned long long>& done)
+{
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 64 || !(attr_set.load() >> dev & 1ull)) {
-        cudaError_t e = cudaFuncSetAttribute(k_forward_brick<M, MODE, SPEC, 4>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (dev < 64 && (done.load() >> dev & 1ull)) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess && dev < 64) done.fetch_or(1ull << dev);
+    return e;
+}
+
+template <int M, int MODE, bool SPEC>
+cudaError_t brick_launch(const MarchParams& prm, const BrickMaps* maps, dim3 grid, size_t smem_loads, size_t smem_tma,
+                         cudaStream_t st)
+{
+    static std::atomic<unsigned long long> set_loads{0}, set_tma{0};
+    if (maps) {
+        const cudaError_t e = opt_in_smem(k_forward_brick_tma<M, MODE, SPEC, 4>, set_tma);
         if (e != cudaSuccess) return e;
-        if (dev < 64) attr_set.fetch_or(1ull << dev);
+        k_forward_brick_tma<M, MODE, SPEC, 4><<<grid, dim3(kBU, kBV), smem_tma, st>>>(prm, *maps);
+    } else {
+        const cudaError_t e = opt_in_smem(k_forward_brick<M, MODE, SPEC, 4>, set_loads);
+        if (e != cudaSuccess) return e;
+        k_forward_brick<M, MODE, SPEC, 4><<<grid, dim3(kBU, kBV), smem_loads, st>>>(prm);
     }
-    k_forward_brick<M, MODE, SPEC, 4><<<grid, dim3(kBU, kBV), smem, st>>>(prm);
     return cudaGetLastError();
 }
 
 template <int M>
-cudaError_t brick_dispatch(const MarchParams& prm, int interp, bool spec, dim3 grid, size_t smem, cudaStream_t st)
+cudaError_t brick_dispatch(const MarchParams& prm, int interp, bool spec, const BrickMaps* maps, dim3 grid,
+                           size_t smem_loads, size_t smem_tma, cudaStream_t st)
 {
     if (interp == INTERP_TRILINEAR)
-        return spec ? brick_launch<M, INTERP_TRILINEAR, true>(prm, grid, smem, st)
-                    : brick_launch<M, INTERP_TRILINEAR, false>(prm, grid, smem, st);
+        return spec ? brick_launch<M, INTERP_TRILINEAR, true>(prm, maps, grid, smem_loads, smem_tma, st)
+                    : brick_launch<M, INTERP_TRILINEAR, false>(prm, maps, grid, smem_loads, smem_tma, st);
     if (interp == INTERP_TEXEMU)
-        return spec ? brick_launch<M, INTERP_TEXEMU, true>(prm, grid, smem, st)
-                    : brick_launch<M, INTERP_TEXEMU, false>(prm, grid, smem, st);
+        return spec ? brick_launch<M, INTERP_TEXEMU, true>(prm, maps, grid, smem_loads, smem_tma, st)
+                    : brick_launch<M, INTERP_TEXEMU, false>(prm, maps, grid, smem_loads, smem_tma, st);
     return cudaErrorInvalidValue;
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    return fn;
+}
+
+// Tensor maps of the M volumes for the TMA-staged boxes, when the volumes
+// allow them: rows of a multiple of 16 bytes (pNumX % 4 == 0) and every base
+// address on a 16-byte boundary.  False: stage with plain loads.
+bool brick_maps(const MarchParams& prm, int M, BrickMaps& bm)
+{
+    const char* mode = std::getenv("CTFP_BRICK_STAGING");
+    if (mode && std::strcmp(mode, "loads") == 0) return false;
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const int nx = prm.g.nx, ny = prm.g.ny, nz = prm.g.nz;
+    if (nx % 4 != 0) return false;
+    std::memset(&bm, 0, sizeof(bm));
+    for (int m = 0; m < M; m++) {
+        if (reinterpret_cast<uintptr_t>(prm.vol[m]) % 16 != 0) return false;
+        const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(float), (cuuint64_t)nx * ny * sizeof(float)};
+        const cuuint32_t box[3] = {(cuuint32_t)kTX, (cuuint32_t)kBY, (cuuint32_t)kBZ};
+        const cuuint32_t estride[3] = {1, 1, 1};
+        if (fn(&bm.tm[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(prm.vol[m]), dims, strides, box,
+               estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
 }
 
 template <int M, int MODE, int SAMPLER, int MINB>
@@ -614,12 +873,16 @@ cudaError_t launch_forward_once(const MarchParams& prm, int M, int interp, int s
         const dim3 grid((prm.g.U + kBU - 1) / kBU, (prm.g.V + kBV - 1) / kBV,
                         (prm.n_views + ls.views_per_cta - 1) / ls.views_per_cta);
         if (grid.z == 0) return cudaSuccess;
-        const size_t smem = sizeof(float) * ((size_t)M * kBoxFloats + (do_spectral ? (size_t)prm.E * M : 0));
+        const size_t mu_floats = do_spectral ? (size_t)prm.E * M : 0;
+        const size_t smem = sizeof(float) * ((size_t)M * kBoxFloats + mu_floats);
+        const size_t smem_tma = 128 + sizeof(float) * ((size_t)M * kTBoxFloats + mu_floats);  // + alignment slack
+        BrickMaps bm;
+        const BrickMaps* maps = brick_maps(prm, M, bm) ? &bm : nullptr;
         switch (M) {
-            case 1: return brick_dispatch<1>(prm, interp, do_spectral, grid, smem, st);
-            case 2: return brick_dispatch<2>(prm, interp, do_spectral, grid, smem, st);
-            case 3: return brick_dispatch<3>(prm, interp, do_spectral, grid, smem, st);
-            case 4: return brick_dispatch<4>(prm, interp, do_spectral, grid, smem, st);
+            case 1: return brick_dispatch<1>(prm, interp, do_spectral, maps, grid, smem, smem_tma, st);
+            case 2: return brick_dispatch<2>(prm, interp, do_spectral, maps, grid, smem, smem_tma, st);
+            case 3: return brick_dispatch<3>(prm, interp, do_spectral, maps, grid, smem, smem_tma, st);
+            case 4: return brick_dispatch<4>(prm, interp, do_spectral, maps, grid, smem, smem_tma, st);
         }
         return cudaErrorInvalidValue;
     }

@@ -28,7 +28,12 @@ struct MarchParams {
     int out_view0;                    // view stored at index 0 of I, IAbs, L, Lin, gI, gIAbs (0: full arrays)
     const uint8_t* occ;               // empty-space skipping: brick occupancy (null: march every sample)
     int occ_x, occ_y;                 // bricks along x, y (see launch_occupancy)
+    unsigned* status;                 // plan-owned word; kCtfpStatusWaitTimeout is or-ed in when a bounded wait ran out
+    int wait_limit;                   // polls of a TMA completion before a CTA gives up on staging
 };
+
+// Bits of the plan's device status word (ctfp_plan_check_status).
+constexpr unsigned kCtfpStatusWaitTimeout = 1u;
 
 // Bricks of kOccShift^2 voxels per axis for empty-space skipping.  Brick
 // (bx, by, bz) is marked when any material has a non-zero voxel in

@@ -159,6 +159,17 @@ class Projector:
         """Empty-space skipping for the layered sampler (ctfp_plan_set_skip_empty)."""
         call("ctfp_plan_set_skip_empty", self._h, 1 if enable else 0)
 
+    def check_status(self, raise_on_timeout: bool = False) -> int:
+        """ctfp_plan_check_status: waits for the device, returns and clears
+        the plan's status bits (1: a TMA-staged brick wait ran out; outputs
+        stay correct).  raise_on_timeout raises CtfpError(CTFP_TIMEOUT) then."""
+        flags = C.c_uint32()
+        st = lib().ctfp_plan_check_status(self._h, C.byref(flags))
+        if st == capi.CTFP_TIMEOUT and not raise_on_timeout:
+            return int(flags.value)
+        capi.check(st, "ctfp_plan_check_status")
+        return int(flags.value)
+
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)
 

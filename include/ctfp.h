@@ -91,7 +91,10 @@ typedef enum ctfp_sampler {
     CTFP_SAMPLER_LAYERED = 2,
     /* the caller's linear volumes staged per ray bundle in shared memory: each
      * CTA (8 x 16 rays, one view at a time) copies the voxel box its rays cross
-     * in the next 16 samples and reads corners from there */
+     * in the next 16 samples and reads corners from there.  The copy is one TMA
+     * tensor load per material (cp.async.bulk.tensor) when pNumX is a multiple
+     * of 4 and every volume starts on a 16-byte boundary, else plain loads;
+     * CTFP_BRICK_STAGING=loads forces plain loads. */
     CTFP_SAMPLER_BRICK = 3
 } ctfp_sampler;
 
@@ -142,6 +145,14 @@ ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t 
  * rounding of the compensated sums.  The global and brick samplers march every
  * sample.  No counterpart in the reference. */
 ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* plan, int32_t enable);
+
+/* Waits for the device, then reads and clears the plan's status word: flags
+ * receives its bits (may be NULL).  Returns CTFP_TIMEOUT when a kernel of the
+ * plan gave up a bounded wait since the last check: a CTA of the TMA-staged
+ * brick sampler whose tensor load did not complete within CTFP_WAIT_LIMIT
+ * polls (default 65536) read those samples from the volume instead and stopped
+ * staging, so its outputs are still correct.  No counterpart in the reference. */
+ctfp_status ctfp_plan_check_status(ctfp_plan* plan, uint32_t* flags);
 
 /* Focal spot (CBCTSinMatPolyForwardProj{Grid,NoGrid}::computePolyForwProjFoSp,
  * Source/CBCTSinMatPolyForwardProjGrid.cpp:269-388, CBCTPolyProjGPU.cu:1927-1978):

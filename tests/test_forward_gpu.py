@@ -333,11 +333,15 @@ def test_rays_missing_volume_are_zero(cuda_ok):
 
 @pytest.mark.parametrize("mode", ["trilinear", "texemu"])
 @pytest.mark.parametrize("pitch", [None, 9.0])
-def test_brick_sampler_equals_layered(cuda_ok, mode, pitch):
+@pytest.mark.parametrize("n,staging", [((40, 36, 30), "tma"), ((40, 36, 30), "loads"), ((41, 36, 30), "tma")])
+def test_brick_sampler_equals_layered(cuda_ok, mode, pitch, n, staging, monkeypatch):
     # same corner values, weights and summation order: identical results,
     # whether the bundle's boxes fit (default pitch) or not (rays many voxels
-    # apart: every segment reads the caller's volume instead)
-    d = small_geometry(n=(40, 36, 30), views=5, U=37, V=35, pitch=pitch)
+    # apart: every segment reads the caller's volume instead), and whether the
+    # boxes are staged by TMA tensor loads (pNumX a multiple of 4) or by plain
+    # loads (CTFP_BRICK_STAGING=loads, or pNumX = 41)
+    monkeypatch.setenv("CTFP_BRICK_STAGING", staging)
+    d = small_geometry(n=n, views=5, U=37, V=35, pitch=pitch)
     vols = random_volumes(d, 3, 12)
     S, mu, G, D = spectral_setup(d, 3, 6, 2)
     with Projector(d, 3, mode) as pr:
@@ -346,7 +350,36 @@ def test_brick_sampler_equals_layered(cuda_ok, mode, pitch):
         pr.set_sampler("brick")
         b = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
+        assert pr.check_status() == 0
     assert torch.equal(a["L"], b["L"]) and torch.equal(a["I"], b["I"]) and torch.equal(a["IAbsorb"], b["IAbsorb"])
+
+
+def test_brick_tma_wait_that_runs_out(cuda_ok, monkeypatch):
+    # with CTFP_WAIT_LIMIT=0 every CTA gives up its first TMA wait at once:
+    # it reads the volume instead (identical outputs), waits for the load
+    # still in flight before exiting, and the plan's status reports
+    # CTFP_TIMEOUT once, then reads clear
+    from ct_forward_projection_b200._capi import CTFP_TIMEOUT, CtfpError
+    d = small_geometry(n=(40, 36, 30), views=4, U=37, V=35)
+    vols = random_volumes(d, 2, 13)
+    S, mu, G, D = spectral_setup(d, 2, 5, 3)
+    with Projector(d, 2, "trilinear") as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        a = pr.forward(to_dev(vols), want_L=True)
+        pr.set_sampler("brick")
+        monkeypatch.setenv("CTFP_WAIT_LIMIT", "0")
+        b = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+        with pytest.raises(CtfpError) as e:
+            pr.check_status(raise_on_timeout=True)
+        assert e.value.status == CTFP_TIMEOUT
+        assert pr.check_status() == 0
+        monkeypatch.delenv("CTFP_WAIT_LIMIT")
+        c = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+        assert pr.check_status() == 0
+    for o in (b, c):
+        assert torch.equal(a["L"], o["L"]) and torch.equal(a["I"], o["I"])
 
 
 def _sparse_volumes(d, M, seed):
