@@ -889,9 +889,10 @@ const float* plan_mu(const ctfp_plan* p) { return p->d_mu; }
 const float* plan_W(const ctfp_plan* p) { return p->d_W; }
 LaunchShape& plan_shape(ctfp_plan* p) { return p->shape; }
 cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m) { return p->ltex[m]; }
+cudaTextureObject_t plan_tex(const ctfp_plan* p, int m) { return p->tex[m]; }
 MarchParams plan_march_params(const ctfp_plan* p) { return base_params(p); }
 const ctfp_geometry& plan_geometry(const ctfp_plan* p) { return p->geom; }
-// Copies the caller's volumes into the plan's layered arrays on stream st.
+// Copies the caller's volumes into the plan's sampler arrays (layered or 3D) on stream st.
 ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
 {
     ctfp_status s = check_volumes(p, volumes);

@@ -38,6 +38,7 @@ int plan_energies(const ctfp_plan* p);
 const float* plan_mu(const ctfp_plan* p);
 const float* plan_W(const ctfp_plan* p);
 cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m);
+cudaTextureObject_t plan_tex(const ctfp_plan* p, int m);
 ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t st);
 }  // namespace ctfp
 
@@ -54,7 +55,8 @@ constexpr int kWarps = 2, kThreads = 32 * kWarps;
 // per call.
 struct ItemDesc {
     GeomParams g;
-    cudaTextureObject_t ltex[kMaxM];
+    cudaTextureObject_t ltex[kMaxM];   // layered textures (TRILINEAR, TEXEMU)
+    cudaTextureObject_t tex[kMaxM];    // 3D textures (TEXTURE: the reference's own sampler)
     const float* mu;   // [E][M]
     const float* W;    // [E][V][U]
     int M, E, interp;
@@ -100,13 +102,25 @@ __device__ __forceinline__ Corner batch_corner(const ItemDesc& it, const RaySeg&
     return corner_tex(ref32_coords(it.g, r, i));
 }
 
-// Path integrals of one ray through the layered sampler.
+// Path integrals of one ray: the layered sampler, or in TEXTURE mode the
+// hardware tex3D at the reference's FP32 coordinates (as k_forward).
 template <int M, int MODE>
 __device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s, const RayRef32& r, float* L)
 {
     float acc[M], cmp[M];
 #pragma unroll
     for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
+    if (MODE == INTERP_TEXTURE) {
+#pragma unroll 2
+        for (int i = s.i0; i < s.i1; i++) {
+            const float3 x = ref32_coords(it.g, r, i);
+#pragma unroll
+            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(it.tex[m], x.x, x.y, x.z));
+        }
+#pragma unroll
+        for (int m = 0; m < M; m++) L[m] = it.g.dx * (acc[m] - cmp[m]);
+        return;
+    }
 #pragma unroll 2
     for (int i = s.i0; i < s.i1; i++) {
         const Corner c = batch_corner<MODE>(it, s, r, i);
@@ -186,7 +200,9 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
         g[m] = -gI * S[m] * it.g.dx;
         any |= g[m] != 0.f;
     }
-    if (any) batch_scatter<M, MODE>(it, s, r, g);
+    // TEXTURE: the transpose of the texture unit's weights, which the
+    // emulation reproduces exactly (as ctfp_backward does for such a plan)
+    if (any) batch_scatter<M, MODE == INTERP_TEXTURE ? INTERP_TEXEMU : MODE>(it, s, r, g);
     return res * res;
 }
 
@@ -288,15 +304,22 @@ __global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long
 
 using KernelFn = void (*)(GroupArgs);
 
+template <int M, bool ADJOINT>
+KernelFn kernel_for_m(int interp)
+{
+    if (interp == INTERP_TRILINEAR) return k_batch<M, INTERP_TRILINEAR, ADJOINT>;
+    if (interp == INTERP_TEXEMU) return k_batch<M, INTERP_TEXEMU, ADJOINT>;
+    return k_batch<M, INTERP_TEXTURE, ADJOINT>;
+}
+
 template <bool ADJOINT>
 KernelFn kernel_for(int M, int interp)
 {
-    const bool tri = interp == INTERP_TRILINEAR;
     switch (M) {
-        case 1: return tri ? k_batch<1, INTERP_TRILINEAR, ADJOINT> : k_batch<1, INTERP_TEXEMU, ADJOINT>;
-        case 2: return tri ? k_batch<2, INTERP_TRILINEAR, ADJOINT> : k_batch<2, INTERP_TEXEMU, ADJOINT>;
-        case 3: return tri ? k_batch<3, INTERP_TRILINEAR, ADJOINT> : k_batch<3, INTERP_TEXEMU, ADJOINT>;
-        default: return tri ? k_batch<4, INTERP_TRILINEAR, ADJOINT> : k_batch<4, INTERP_TEXEMU, ADJOINT>;
+        case 1: return kernel_for_m<1, ADJOINT>(interp);
+        case 2: return kernel_for_m<2, ADJOINT>(interp);
+        case 3: return kernel_for_m<3, ADJOINT>(interp);
+        default: return kernel_for_m<4, ADJOINT>(interp);
     }
 }
 
@@ -438,7 +461,7 @@ struct DevScope {
 
 bool batchable(const ctfp_plan* p)
 {
-    return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_LAYERED && !plan_geom(p).fspot;
+    return (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) == SAMPLER_LAYERED) && !plan_geom(p).fspot;
 }
 
 // Fills the per-call tables from the plans' current state.
@@ -448,7 +471,7 @@ ctfp_status fill_items(ctfp_batch* b)
         ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
         if (!batchable(p))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler and no focal spot");
+                         "batched items need the layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
         if (plan_energies(p) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
         ItemDesc& it = b->items[(size_t)s];
         const long long unit0 = it.unit0, units = it.units;
@@ -464,6 +487,7 @@ ctfp_status fill_items(ctfp_batch* b)
         it.W = plan_W(p);
         for (int m = 0; m < it.M; m++) {
             it.ltex[m] = plan_ltex(p, m);
+            it.tex[m] = plan_tex(p, m);
             it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
         }
         it.tiles_u = (it.g.U + kTU - 1) / kTU;
@@ -490,7 +514,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         if (plan_device(plans[i]) != dev) return bfail(CTFP_INVALID_ARG, "plans must share one device");
         if (!batchable(plans[i]))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered sampler and no focal spot");
+                         "batched items need the layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
         if (plan_energies(plans[i]) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
     }
     DevScope ds(dev);

@@ -287,8 +287,10 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * the plans' own texture arrays: do not run a batch and its plans
  * concurrently.
  *
- * Items must use CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU with the layered
- * sampler (the default) and have spectral tables set.  The batch keeps the
+ * Items use the layered sampler (the default) in CTFP_INTERP_TRILINEAR or
+ * CTFP_INTERP_TEXEMU, or CTFP_INTERP_TEXTURE (hardware tex3D; its adjoint is the
+ * transpose of the texture unit's weights, as ctfp_backward), have no focal
+ * spot and have spectral tables set.  The batch keeps the
  * plans' pointers: destroy it before them.  Arrays indexed by item follow the
  * order of `plans`. */
 typedef struct ctfp_batch ctfp_batch;

@@ -175,7 +175,7 @@ def test_fused_log_loss_binding(cuda_ok):
     # LogIntensityLoss (the fused forward + loss + adjoint kernel) gives the
     # loss and gradients of sum (log I - log T)^2 computed through project(),
     # scales its gradient by the incoming one, and replays its graph on a
-    # second call; hardware-texture plans are refused
+    # second call, in the exact and the hardware-texture modes
     from ct_forward_projection_b200._capi import CtfpError
     from ct_forward_projection_b200.autograd import LogIntensityLoss, project
     d = small_geometry(n=(13, 12, 10), views=4, U=14, V=10)
@@ -201,8 +201,23 @@ def test_fused_log_loss_binding(cuda_ok):
                 for m in range(M):
                     err = torch.max(torch.abs(ys[m].grad - 2.0 * xs[m].grad)) / torch.max(torch.abs(2.0 * xs[m].grad))
                     assert float(err) < 1e-5
+    # the reference's own sampler: the same loss and gradients as project()
     with Projector(d, M, "texture") as pt:
         pt.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        xs = [torch.from_numpy(v).cuda().requires_grad_(True) for v in vols]
+        I, _, _ = project(pt, *xs)
+        ref = torch.sum((torch.log(I) - torch.log(T)) ** 2)
+        ref.backward()
+        with LogIntensityLoss(pt) as lf:
+            ys = [torch.from_numpy(v).cuda().requires_grad_(True) for v in vols]
+            loss = lf(T, *ys)
+            loss.backward()
+            torch.cuda.synchronize()
+        assert abs(float(loss.detach()) - float(ref.detach())) <= 1e-5 * abs(float(ref.detach()))
+        for m in range(M):
+            assert float(torch.max(torch.abs(ys[m].grad - xs[m].grad)) / torch.max(torch.abs(xs[m].grad))) < 1e-5
+        # a plan with a focal spot has no adjoint
+        pt.set_focal_spot(np.full(d["projNum"], 0.1, np.float32), np.zeros(d["projNum"], np.float32))
         with pytest.raises(CtfpError):
             LogIntensityLoss(pt)
 

@@ -1,6 +1,6 @@
 """The batched form (ctfp_batch_*; no reference counterpart): persistent
 kernels over a work queue of (item, view, 8 x 8 ray tile) units, replayed as
-a CUDA graph.  Every item's outputs must equal the plain per-plan calls on the same
+a CUDA graph; items in every interpolation mode, the hardware texture included.  Every item's outputs must equal the plain per-plan calls on the same
 inputs; the fused forward + loss + adjoint must equal ctfp_forward followed by
 ctfp_backward with dLoss/dI formed on the host."""
 import numpy as np
@@ -20,6 +20,7 @@ ITEMS = [
     dict(n=(12, 12, 12), views=3, U=13, V=9, M=1, E=4, mode="texemu", seed=2),
     dict(n=(26, 18, 9), views=7, U=33, V=17, M=3, E=11, mode="trilinear", seed=3),
     dict(n=(9, 11, 14), views=2, U=8, V=8, M=4, E=5, mode="texemu", seed=4),
+    dict(n=(16, 14, 12), views=4, U=19, V=13, M=2, E=6, mode="texture", seed=5),
 ]
 
 
@@ -131,14 +132,22 @@ def test_batch_forward_adjoint_equals_plain(cuda_ok, specs):
     b.close()
 
 
-def test_batch_rejects_texture_mode_and_missing_tables(cuda_ok):
+def test_batch_rejects_focal_spot_other_samplers_and_missing_tables(cuda_ok):
     d = small_geometry(n=8, views=2, U=8, V=8)
+    S, mu, G, D = spectral_setup(d, 1, 3, 1)
     with Projector(d, 1, "texture") as pr:
-        S, mu, G, D = spectral_setup(d, 1, 3, 1)
         pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_focal_spot(np.full(2, 0.1, np.float32), np.zeros(2, np.float32))
         with pytest.raises(CtfpError) as e:
             Batch([pr])
         assert e.value.status == CTFP_UNSUPPORTED
+    for sampler in ("global", "brick"):
+        with Projector(d, 1, "trilinear") as pr:
+            pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+            pr.set_sampler(sampler)
+            with pytest.raises(CtfpError) as e:
+                Batch([pr])
+            assert e.value.status == CTFP_UNSUPPORTED
     with Projector(d, 1, "trilinear") as pr:
         with pytest.raises(CtfpError) as e:
             Batch([pr])
