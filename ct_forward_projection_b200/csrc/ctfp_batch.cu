@@ -79,6 +79,7 @@ struct GroupArgs {
     int first, count;
     long long begin, end;
     unsigned long long* counter;
+    int tu_shift;  // rays of a unit (one view): (1 << tu_shift) x (kThreads >> tu_shift)
 };
 
 __device__ __forceinline__ int find_item(const GroupArgs& a, long long unit)
@@ -261,8 +262,8 @@ __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb)
             tv = t / it.tiles_u;
             tu = t % it.tiles_u;
         }
-        const int u = tu * kTU + (threadIdx.x % kTU);
-        const int v = tv * kTV + (threadIdx.x / kTU);
+        const int u = (tu << a.tu_shift) + (threadIdx.x & ((1 << a.tu_shift) - 1));
+        const int v = tv * (kThreads >> a.tu_shift) + (threadIdx.x >> a.tu_shift);
         float loss = 0.f;
         if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT>(it, s_mu, p, v, u);
         if (ADJOINT && it.loss) {
@@ -328,6 +329,7 @@ KernelFn kernel_for(int M, int interp)
 struct ctfp_batch {
     int n = 0;
     int device = 0;
+    int tile_u = kTU, tile_v = kTV;  // rays of a work unit (ctfp_batch_set_shape / ctfp_batch_autotune)
     std::vector<ctfp_plan*> plans;
     std::vector<int> order;            // item slot -> plan index (grouped, cost order within a group)
     std::vector<long long> vox0;       // first voxel of each slot in the fold's flat index
@@ -375,10 +377,11 @@ ctfp_status bfail(ctfp_status st, const std::string& m)
 
 // Records one call's stream work: volume uploads, counters, accumulators, the
 // persistent kernel of every group, the fold.
-ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vols, float* loss, cudaStream_t st)
+ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>& vols, float* loss, cudaStream_t st,
+                   int tune_div = 0)
 {
     size_t off = 0;
-    for (int s = 0; s < b->n; s++) {
+    for (int s = 0; s < b->n && tune_div == 0; s++) {
         ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
         ctfp_status rs = plan_upload(p, vols.data() + off, st);
         if (rs != CTFP_OK) return rs;
@@ -386,18 +389,21 @@ ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>&
     }
     BATCH_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * b->groups.size(), st));
     if (adjoint) {
-        BATCH_CUDA(cudaMemsetAsync(b->d_gexp, 0, b->gexp_elems * sizeof(float4), st));
+        // (tuning leaves the accumulators as they are: a real call zeroes them)
+        if (tune_div == 0) BATCH_CUDA(cudaMemsetAsync(b->d_gexp, 0, b->gexp_elems * sizeof(float4), st));
         if (loss) BATCH_CUDA(cudaMemsetAsync(loss, 0, sizeof(float) * (size_t)b->n, st));
     }
     const ItemDesc* table = b->d_items[adjoint ? 1 : 0];
     for (size_t gi = 0; gi < b->groups.size(); gi++) {
         const ctfp_batch::Group& G = b->groups[gi];
-        GroupArgs a{table, G.first, G.count, G.begin, G.end, b->d_counter + gi};
+        // tuning runs the first 1/tune_div of each group's queue: its largest items
+        const long long end = tune_div > 0 ? G.begin + std::max(1LL, (G.end - G.begin) / tune_div) : G.end;
+        GroupArgs a{table, G.first, G.count, G.begin, end, b->d_counter + gi, __builtin_ctz((unsigned)b->tile_u)};
         KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp) : kernel_for<false>(G.M, G.interp);
         fn<<<G.grid[adjoint ? 1 : 0], kThreads, 0, st>>>(a);
         BATCH_CUDA(cudaGetLastError());
     }
-    if (adjoint) {
+    if (adjoint && tune_div == 0) {
         long long nb = (b->total_vox + 255) / 256;
         if (nb > 148 * 16) nb = 148 * 16;
         k_batch_fold<<<(unsigned)std::max<long long>(nb, 1), 256, 0, st>>>(table, b->n, b->d_vox0, b->total_vox);
@@ -464,6 +470,25 @@ bool batchable(const ctfp_plan* p)
     return (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) == SAMPLER_LAYERED) && !plan_geom(p).fspot;
 }
 
+// Unit counts and queue ranges for the batch's unit shape: item s holds
+// tiles_u x tiles_v x P units, numbered after the items before it.
+void layout_units(ctfp_batch* b)
+{
+    long long unit = 0;
+    size_t gi = 0;
+    for (int s = 0; s < b->n; s++) {
+        const GeomParams& g = plan_geom(b->plans[(size_t)b->order[(size_t)s]]);
+        ItemDesc& it = b->items[(size_t)s];
+        while (gi + 1 < b->groups.size() && s >= b->groups[gi + 1].first) gi++;
+        if (s == b->groups[gi].first) b->groups[gi].begin = unit;
+        it.unit0 = unit;
+        it.units = (long long)((g.U + b->tile_u - 1) / b->tile_u) * ((g.V + b->tile_v - 1) / b->tile_v) * g.P;
+        unit += it.units;
+        b->groups[gi].end = unit;
+    }
+    b->total_units = unit;
+}
+
 // Fills the per-call tables from the plans' current state.
 ctfp_status fill_items(ctfp_batch* b)
 {
@@ -490,8 +515,8 @@ ctfp_status fill_items(ctfp_batch* b)
             it.tex[m] = plan_tex(p, m);
             it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
         }
-        it.tiles_u = (it.g.U + kTU - 1) / kTU;
-        it.tiles_v = (it.g.V + kTV - 1) / kTV;
+        it.tiles_u = (it.g.U + b->tile_u - 1) / b->tile_u;
+        it.tiles_v = (it.g.V + b->tile_v - 1) / b->tile_v;
         it.unit0 = unit0;
         it.units = units;
     }
@@ -552,13 +577,9 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         ItemDesc& it = b->items[(size_t)s];
         it.M = plan_materials(p);
         it.interp = plan_interp(p);
-        it.unit0 = unit;
-        it.units = (long long)((g.U + kTU - 1) / kTU) * ((g.V + kTV - 1) / kTV) * g.P;
         if (b->groups.empty() || b->groups.back().M != it.M || b->groups.back().interp != it.interp)
             b->groups.push_back({it.M, it.interp, s, 0, unit, unit, {0, 0}});
         b->groups.back().count++;
-        unit += it.units;
-        b->groups.back().end = unit;
         b->vox0[(size_t)s] = vox;
         vox += (long long)g.nx * g.ny * g.nz;
         for (int m = 0; m < it.M; m++) {
@@ -566,7 +587,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
             gexp += expanded_elems(g);
         }
     }
-    b->total_units = unit;
+    layout_units(b);
     b->total_vox = vox;
     b->gexp_elems = gexp;
     cudaError_t e = cudaMalloc(&b->d_items[0], sizeof(ItemDesc) * (size_t)n_items);
@@ -663,6 +684,108 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* b, const float* const* const*
         it.loss = loss ? loss + k : nullptr;
     }
     return run(b, true, vols, loss, (cudaStream_t)stream);
+}
+
+ctfp_status ctfp_batch_set_shape(ctfp_batch* b, int32_t tile_u, int32_t tile_v)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (tile_u < 1 || tile_v < 1 || tile_u * tile_v != kThreads || (tile_u & (tile_u - 1)) != 0)
+        return bfail(CTFP_INVALID_ARG, "tile_u x tile_v must be 64 rays, tile_u a power of two");
+    DevScope ds(b->device);
+    // graphs recorded with the old queue may still be running
+    BATCH_CUDA(cudaDeviceSynchronize());
+    for (ctfp_batch::Graph& G : b->graph) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+    }
+    b->tile_u = tile_u;
+    b->tile_v = tile_v;
+    layout_units(b);
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volumes, const float* const* I_target,
+                                ctfp_launch_shape* out, void* stream)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (!volumes || !I_target) return bfail(CTFP_INVALID_ARG, "volumes and I_target are required");
+    DevScope ds(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<const float*> vols;
+    for (int s = 0; s < b->n; s++) {
+        const int k = b->order[(size_t)s];
+        if (!volumes[k] || !I_target[k]) return bfail(CTFP_INVALID_ARG, "NULL volume list or target for an item");
+        for (int m = 0; m < b->items[(size_t)s].M; m++) vols.push_back(volumes[k][m]);
+    }
+    // the volumes once into the plans' arrays; the candidates then time only
+    // their kernels, on the first eighth of every group's queue
+    size_t off = 0;
+    for (int s = 0; s < b->n; s++) {
+        ctfp_status rs = plan_upload(b->plans[(size_t)b->order[(size_t)s]], vols.data() + off, st);
+        if (rs != CTFP_OK) return rs;
+        off += (size_t)b->items[(size_t)s].M;
+    }
+    float* loss = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BATCH_CUDA(cudaMalloc(&loss, sizeof(float) * (size_t)b->n));
+    struct Freer {
+        float* p;
+        cudaEvent_t a, c;
+        ~Freer()
+        {
+            cudaFree(p);
+            if (a) cudaEventDestroy(a);
+            if (c) cudaEventDestroy(c);
+        }
+    } freer{loss, nullptr, nullptr};
+    BATCH_CUDA(cudaEventCreate(&e0));
+    freer.a = e0;
+    BATCH_CUDA(cudaEventCreate(&e1));
+    freer.c = e1;
+    static const int shapes[][2] = {{8, 8}, {16, 4}, {4, 16}, {32, 2}, {2, 32}};
+    const int keep[2] = {b->tile_u, b->tile_v};
+    int best = -1;
+    float best_ms = 0.f;
+    for (int c = 0; c < (int)(sizeof(shapes) / sizeof(shapes[0])); c++) {
+        b->tile_u = shapes[c][0];
+        b->tile_v = shapes[c][1];
+        layout_units(b);
+        ctfp_status rs = fill_items(b);
+        if (rs != CTFP_OK) return rs;
+        for (int s = 0; s < b->n; s++) {
+            ItemDesc& it = b->items[(size_t)s];
+            it.I_target = I_target[b->order[(size_t)s]];
+            it.loss = loss + b->order[(size_t)s];
+        }
+        BATCH_CUDA(cudaStreamSynchronize(st));
+        BATCH_CUDA(cudaMemcpy(b->d_items[1], b->items.data(), sizeof(ItemDesc) * (size_t)b->n, cudaMemcpyHostToDevice));
+        rs = record(b, true, vols, loss, st, 8);  // warm-up
+        if (rs != CTFP_OK) return rs;
+        BATCH_CUDA(cudaEventRecord(e0, st));
+        rs = record(b, true, vols, loss, st, 8);
+        if (rs != CTFP_OK) return rs;
+        BATCH_CUDA(cudaEventRecord(e1, st));
+        BATCH_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (best < 0 || ms < best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    b->tile_u = keep[0];
+    b->tile_v = keep[1];
+    const ctfp_status rs = ctfp_batch_set_shape(b, shapes[best][0], shapes[best][1]);
+    if (rs != CTFP_OK) return rs;
+    if (out) {
+        out->tile_u = shapes[best][0];
+        out->tile_v = shapes[best][1];
+        out->views_per_cta = 1;
+        out->min_ctas_per_sm = 0;
+        out->ms = best_ms;
+        out->from_cache = 0;
+    }
+    return CTFP_OK;
 }
 
 ctfp_status ctfp_batch_info(const ctfp_batch* b, int64_t* total_units, int32_t* grid_forward, int32_t* grid_adjoint)

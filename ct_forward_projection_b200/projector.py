@@ -343,6 +343,19 @@ class Batch:
         except Exception:
             pass
 
+    def set_shape(self, tile_u: int, tile_v: int) -> None:
+        """ctfp_batch_set_shape: tile_u x tile_v (= 64) rays per work unit."""
+        call("ctfp_batch_set_shape", self._h, tile_u, tile_v)
+
+    def autotune(self, volumes: Sequence[Sequence], targets: Sequence, stream=None) -> dict:
+        """ctfp_batch_autotune: times the fused kernels with candidate unit shapes, keeps the fastest."""
+        self._keep = []
+        vt = self._vol_table(volumes)
+        T = self._item_ptrs(targets, 1, "target")
+        r = capi.LaunchShape()
+        call("ctfp_batch_autotune", self._h, vt, T, C.byref(r), _stream(stream))
+        return {"tile_u": r.tile_u, "tile_v": r.tile_v, "ms": r.ms}
+
     def info(self) -> dict:
         u, g0, g1 = C.c_int64(), C.c_int32(), C.c_int32()
         call("ctfp_batch_info", self._h, C.byref(u), C.byref(g0), C.byref(g1))

@@ -277,7 +277,8 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
  * spectral tables; one device) and runs them with persistent kernels over a
  * device work queue: a work unit is one view x one 8 x 8 detector tile (the
- * 64 rays of one CTA); items are grouped by material count and sampler mode
+ * 64 rays of one CTA; see ctfp_batch_set_shape and ctfp_batch_autotune for
+ * other shapes); items are grouped by material count and sampler mode
  * (one kernel per group, each with its own register budget) and queued
  * largest first (rays x samples x materials); every CTA takes the next unit
  * from an atomic counter.  A call is recorded once as a CUDA graph (volume
@@ -313,6 +314,20 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* co
                                        float* const* const* g_volumes, float* loss, void* stream);
 
 /* Work units in the queue, persistent grid sizes of the two kernels. */
+/* Ray tile of a work unit (one view): tile_u x tile_v rays, whose product must
+ * be 64, the threads of a persistent CTA, with tile_u a power of two (default
+ * 8 x 8).  Waits for the
+ * device; the next call re-records its graph.  (A unit holds one view: a
+ * runtime loop over several views cost the persistent kernels spills.) */
+ctfp_status ctfp_batch_set_shape(ctfp_batch* batch, int32_t tile_u, int32_t tile_v);
+/* Times the fused forward + loss + adjoint kernels with candidate ray tiles
+ * (8 x 8, 16 x 4, 4 x 16, 32 x 2, 2 x 32) on the first eighth of every group's
+ * work queue (its largest problems) and keeps the fastest.  Reads volumes and
+ * I_target as ctfp_batch_forward_adjoint does and writes nothing the caller
+ * owns; out (may be NULL) receives tile_u, tile_v, views_per_cta = 1 and ms.
+ * Waits for the device. */
+ctfp_status ctfp_batch_autotune(ctfp_batch* batch, const float* const* const* volumes, const float* const* I_target,
+                                ctfp_launch_shape* out, void* stream);
 ctfp_status ctfp_batch_info(const ctfp_batch* batch, int64_t* total_units, int32_t* grid_forward,
                             int32_t* grid_adjoint);
 

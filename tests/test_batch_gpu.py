@@ -152,3 +152,48 @@ def test_batch_rejects_focal_spot_other_samplers_and_missing_tables(cuda_ok):
         with pytest.raises(CtfpError) as e:
             Batch([pr])
         assert e.value.status == CTFP_NOT_READY
+
+
+@pytest.mark.parametrize("shape", [(16, 4), (4, 16), (32, 2), (64, 1)])
+def test_batch_unit_shapes_equal_plain_calls(cuda_ok, shape):
+    # any ray tile covers every ray of every view exactly once
+    items = make_items(ITEMS)
+    b = Batch([it[0] for it in items])
+    b.set_shape(*shape)
+    tu, tv = shape
+    assert b.info()["units"] == sum(((sp["U"] + tu - 1) // tu) * ((sp["V"] + tv - 1) // tv) * sp["views"]
+                                    for sp in ITEMS)
+    with pytest.raises(CtfpError):
+        b.set_shape(8, 4)
+    outs = b.forward([it[1] for it in items], want_L=True)
+    torch.cuda.synchronize()
+    for (pr, vols, _), o in zip(items, outs):
+        ref = pr.forward(vols, want_L=True)
+        torch.cuda.synchronize()
+        assert rel(o["I"], ref["I"]) < 2e-6 and rel(o["L"], ref["L"]) < 1e-6
+    b.close()
+
+
+def test_batch_autotune_keeps_results(cuda_ok):
+    # the tuner changes only the unit shape: the fused step afterwards equals
+    # the plain calls, and nothing the caller owns was written while tuning
+    items = make_items(ITEMS)
+    targets, ref_grads = [], []
+    for pr, vols, _ in items:
+        f = pr.forward(vols, want_L=True)
+        T = (f["I"] * 1.03).contiguous()
+        targets.append(T)
+        r = torch.log(f["I"].double()) - torch.log(T.double())
+        ref_grads.append(pr.backward(f["L"], gI=(2.0 * r / f["I"].double()).float()))
+    torch.cuda.synchronize()
+    b = Batch([it[0] for it in items])
+    grads = [[torch.zeros_like(v) for v in it[1]] for it in items]
+    shape = b.autotune([it[1] for it in items], targets)
+    assert shape["tile_u"] * shape["tile_v"] == 64 and shape["ms"] > 0
+    assert all(float(g.abs().max()) == 0.0 for gk in grads for g in gk)
+    res = b.forward_adjoint([it[1] for it in items], targets, grads=grads)
+    torch.cuda.synchronize()
+    for k, (pr, _, _) in enumerate(items):
+        for m in range(pr.M):
+            assert rel(res["grads"][k][m], ref_grads[k][m]) < 1e-4
+    b.close()
