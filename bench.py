@@ -598,6 +598,8 @@ def batch_leg(args, ws, rank, local, stream):
         pr.forward(v, out=o)
         targets.append(o["I"] * torch.exp(0.05 * torch.randn(o["I"].shape, device=dev, generator=gen)))
     b = Batch(prs)
+    # the work-unit ray tile, tuned on the fused kernels (untimed)
+    unit_shape = b.autotune(vols, targets)
     b_outs = [{"I": torch.empty_like(o["I"]), "IAbsorb": torch.empty_like(o["I"])} for o in outs]
     b_I = [torch.empty_like(o["I"]) for o in outs]
     loss_b = torch.zeros(len(prs), device=dev)
@@ -662,6 +664,7 @@ def batch_leg(args, ws, rank, local, stream):
     return {
         "items": len(wl), "rays_per_pass": rays, "work_units": info["units"],
         "persistent_grid": [info["grid_forward"], info["grid_adjoint"]],
+        "unit_tile": [unit_shape["tile_u"], unit_shape["tile_v"]],
         "fwd": {"loop_rays_s": n_rays / (t_loop_f / 1e3), "batched_rays_s": n_rays / (t_b_f / 1e3),
                 "loop_ms": t_loop_f, "batched_ms": t_b_f, "speedup": t_loop_f / t_b_f},
         "fwd_adjoint": {"loop_rays_s": n_rays / (t_loop_fa / 1e3), "batched_rays_s": n_rays / (t_b_fa / 1e3),
