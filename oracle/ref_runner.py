@@ -195,16 +195,3 @@ def reference_case_from_workload(w, g: dict) -> dict:
                  "inter_ma": physics.mass_attenuation(w.grid.inter_material, energies)},
     }
 
-
-if __name__ == "__main__":
-    # one run of the reference binary on a named workload with fewer views:
-    #   python -m oracle.ref_runner poly_grid_256 8
-    import sys
-
-    from ct_forward_projection_b200 import physics
-    w = physics.workload(sys.argv[1] if len(sys.argv) > 1 else "poly_grid_256")
-    g = dict(w.geometry)
-    g["projNum"] = int(sys.argv[2]) if len(sys.argv) > 2 else 8
-    _, dt, _ = run(reference_case_from_workload(w, g), timeout=900)
-    print(f"reference run: {g['projNum']} views, {dt:.3f} s wall, "
-          f"{g['projNum'] * g['dNumU'] * g['dNumV'] / dt:.4g} rays/s", flush=True)
