@@ -216,6 +216,12 @@ def _cpu_model() -> str:
     return "unknown"
 
 
+def _ref_runner():
+    """oracle/ref_runner (the package module, whatever was imported before)."""
+    from oracle import ref_runner
+    return ref_runner
+
+
 def reference_arm(args, w, ws, rank):
     """The reference's own implementation of the path.  Its projector is CUDA
     (Source/CUDAFun/CBCTPolyProjGPU.cu); oracle/build_ref.sh builds it from the
@@ -225,9 +231,7 @@ def reference_arm(args, w, ws, rank):
         return None
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ctfp_ref")
     if os.path.exists(ref_bin):
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        from oracle import ref_runner
-        return ref_runner.bench_line(args, w)
+        return _ref_runner().bench_line(args, w)
     from oracle import oracle as O
     g = w.geometry
     rng = np.random.RandomState(7)

@@ -61,3 +61,13 @@ def test_reference_arm_other_ranks_exit_at_once():
                         "reference", "--gpus", "2"], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_finds_its_runner_in_a_fresh_process():
+    # the reference arm imports oracle/ref_runner before anything else has
+    # imported the oracle package
+    import subprocess
+    code = "import bench; r = bench._ref_runner(); assert r.REF_BIN.endswith('ctfp_ref')"
+    r = subprocess.run([sys.executable, "-c", code], cwd=os.path.dirname(bench.__file__), capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
