@@ -71,3 +71,32 @@ def test_reference_arm_finds_its_runner_in_a_fresh_process():
     r = subprocess.run([sys.executable, "-c", code], cwd=os.path.dirname(bench.__file__), capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+def test_cpu_baseline_accuracy_figures():
+    # the bench's accuracy block on a small problem whose "GPU" outputs are the
+    # oracle's own, rounded to float32: per-ray errors at FP32 rounding, the
+    # projection error likewise, and the sample sized from the time budget
+    import types
+
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from tests.conftest import random_volumes, small_geometry, spectral_setup
+    d = small_geometry(n=(16, 16, 16), views=4, U=20, V=10)
+    vols = random_volumes(d, 2, 3)
+    S, mu, G, D = spectral_setup(d, 2, 6, 11)
+    W = O.energy_weights(d, S, G, 2, D, 1000.0)
+    n = 4 * 20 * 10
+    w = types.SimpleNamespace(geometry=d, n_rays=n, _vols=[torch.from_numpy(v) for v in vols], _W=W,
+                              mu_table=lambda: mu)
+    ref = O.forward(d, vols, mu, W, O.TRILINEAR, np.arange(n))
+    gpu = {"I": ref["I"].astype(np.float32), "IAbsorb": ref["IAbsorb"].astype(np.float32),
+           "I0": ref["I0"].astype(np.float32)}
+    cpu, acc = bench.cpu_baseline(w, gpu, 0.2)
+    assert cpu["kind"] == "port" and cpu["value"] > 0 and cpu["cores"] >= 1
+    for k in ("I", "IAbsorb", "I0"):
+        assert acc[k]["max"] < 1e-7 and acc[k]["p99"] <= acc[k]["max"]
+    assert acc["proj_abs"]["max"] < 1e-3
+    assert acc["rays"] == n
