@@ -1,6 +1,7 @@
 """View sharding of one object across ranks (ct_forward_projection_b200.shard),
-host logic on CPU: two `gloo` ranks, each with a stand-in projector that
-computes its view range with the FP64 oracle (test infrastructure), must give
+host logic on CPU: two and three `gloo` ranks (7 views in slabs of 4 + 3 and
+3 + 2 + 2), each with a stand-in projector that computes its view range with
+the FP64 oracle (test infrastructure), must give
 the single-process projection (all-gather) and gradient (all-reduce)."""
 import os
 import socket
@@ -103,7 +104,7 @@ def _free_port():
     return port
 
 
-@pytest.mark.parametrize("world", [2])
+@pytest.mark.parametrize("world", [2, 3])
 def test_view_sharded_forward_and_adjoint_match_one_process(world):
     with tempfile.TemporaryDirectory() as td:
         mp.start_processes(_rank_main, args=(world, _free_port(), td), nprocs=world, join=True, start_method="spawn")
