@@ -622,6 +622,114 @@ int orc_grid_column(int64_t dNumU, float dSize_mm, int strip_um, int inter_um, f
     return 0;
 }
 
+/* The 1-um unit pattern of the focused grid, unit by unit, as the fill loops
+ * of Grid::createDiscreteGrid_u{E,O}d{E,O} lay it out (Grid.cpp:90-270):
+ * kind[i] = 1 for a lead-strip unit, 0 for an interspace unit, -1 for a unit
+ * no loop writes (none for valid widths; it would transmit 0); src[i] = the
+ * unit whose height sets unit i's path length -- its own, except interspace
+ * units of the periodic region, which take their period's first unit
+ * (Grid.cpp:115, 160, 203, 249).  Units right of the mirror take kind and
+ * source of their mirror images (Grid.cpp:126-129, 170-173, 214-217,
+ * 260-263).  Returns -1 when the detector is narrower than the central
+ * interspace (the reference's size_t loops would wrap). */
+static int grid_pattern(size_t N, int strip_um, int inter_um, signed char* kind, int64_t* src)
+{
+    const int period = strip_um + inter_um;
+    if (N < (size_t)inter_um + 2 || strip_um <= 0 || inter_um <= 0) return -1;
+    for (size_t i = 0; i < N; i++) { kind[i] = -1; src[i] = (int64_t)i; }
+    const int uOdd = (int)(N % 2), iOdd = inter_um % 2;
+    const int64_t c = (int64_t)(N / 2), half = inter_um / 2;
+    int64_t start;
+    /* the central interspace half-gap, each unit at its own height */
+    if (!uOdd) {
+        if (iOdd) kind[c] = 0;                          /* uEdO: Grid.cpp:137 */
+        for (int64_t i = c - 1; i > c - 1 - half; i--) kind[i] = 0;
+        start = c - 1 - half;
+    } else if (!iOdd) {
+        for (int64_t i = c; i > c - half; i--) kind[i] = 0; /* uOdE: Grid.cpp:181-184 */
+        start = c - half;
+    } else {
+        kind[c] = 0;                                    /* uOdO: Grid.cpp:226 */
+        for (int64_t i = c - 1; i > c - 1 - half; i--) kind[i] = 0;
+        start = c - 1 - half;
+    }
+    /* periods counted leftwards from start: strip units, then interspace
+     * units that all take the height of the period's first unit */
+    for (int64_t i = start; i >= 0; i -= period) {
+        for (int k = 0; k < strip_um && i - k >= 0; k++) { kind[i - k] = 1; src[i - k] = i - k; }
+        for (int k = 0; k < inter_um && i - strip_um - k >= 0; k++) {
+            kind[i - strip_um - k] = 0;
+            src[i - strip_um - k] = i;
+        }
+    }
+    /* mirror: the first unit of the right half and the image of unit i */
+    const int64_t m0 = (!uOdd && !iOdd) ? c : c + 1;
+    const int minus1 = (!uOdd && !iOdd) || (uOdd && iOdd);
+    for (int64_t i = m0; i < (int64_t)N; i++) {
+        const int64_t j = minus1 ? (int64_t)N - i - 1 : (int64_t)N - i;
+        kind[i] = kind[j];
+        src[i] = src[j];
+    }
+    return 0;
+}
+
+/* Per-pixel, per-energy grid transmission from the incidence angle, FP64,
+ * unit by unit.  The focused strips of Grid::defGrid / updataGrid
+ * (Grid.cpp:373-443) are parallel to the detector's v axis and converge on the
+ * focal line at distance FD, so a ray into row v crosses each 1-um unit along
+ * a path of length h / FD * sqrt(FD^2 + d^2 + y^2): the reference's unit height
+ * h / FD * sqrt(FD^2 + d^2) (Grid.cpp:76-87) with y, the row centre's offset
+ * from the detector centre (row 0 at +dHalfLV - dSize / 2, as the ray geometry
+ * CBCTPolyProjGPU.cu:1813-1814 places it), added under the root.  Each unit
+ * transmits exp(-mu * height at its source unit) (grid_pattern), and pixel u
+ * of row v is the mean over its dSize units, summed in double (Grid.cpp:297-309).
+ * Widths in um, h, FD and dSize in mm, attenuation in 1/mm; the per-pixel unit
+ * count dSize is the reference's truncation of dSize_mm * 1000 to integer um
+ * (CBCTPolyForwardProjGrid.cpp:291).  Only the rows listed are built:
+ * out[e][r][u] for rows[r], r < n_rows.  OpenMP over (energy, row). */
+int orc_grid_pixel(int64_t dNumU, int64_t dNumV, float dSize_mm, int strip_um, int inter_um, float h_mm, float FD_mm,
+                   int E, const float* mu_strip_mm, const float* mu_inter_mm, int64_t n_rows, const int64_t* rows,
+                   double* out)
+{
+    const size_t dSize = (size_t)(float)(dSize_mm * 1000);
+    const size_t N = (size_t)dNumU * dSize;
+    if (dSize == 0 || dNumU <= 0 || dNumV <= 0) return -1;
+    for (int64_t r = 0; r < n_rows; r++)
+        if (rows[r] < 0 || rows[r] >= dNumV) return -1;
+    signed char* kind = (signed char*)malloc(N);
+    int64_t* src = (int64_t*)malloc(N * sizeof(int64_t));
+    if (grid_pattern(N, strip_um, inter_um, kind, src) != 0) {
+        free(kind);
+        free(src);
+        return -1;
+    }
+    const double h = (double)h_mm * 1000.0, FD = (double)FD_mm * 1000.0, dsz = (double)dSize_mm * 1000.0;
+    const double halfN = (double)N / 2.0;
+    int rc = 0;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+    for (int e = 0; e < E; e++) {
+        for (int64_t r = 0; r < n_rows; r++) {
+            const double y = (double)dNumV * dsz / 2.0 - dsz / 2.0 - (double)rows[r] * dsz;
+            const double ms = (double)mu_strip_mm[e] / 1000.0, mi = (double)mu_inter_mm[e] / 1000.0;
+            double* o = out + ((int64_t)e * n_rows + r) * dNumU;
+            for (int64_t u = 0; u < dNumU; u++) {
+                double sum = 0.0;
+                for (size_t k = 0; k < dSize; k++) {
+                    const size_t i = (size_t)u * dSize + k;
+                    if (kind[i] < 0) continue;
+                    const double d = (double)src[i] + 0.5 - halfN;
+                    const double H = h / FD * sqrt(FD * FD + d * d + y * y);
+                    sum += exp(-(kind[i] ? ms : mi) * H);
+                }
+                o[u] = sum / (double)dSize;
+            }
+        }
+    }
+    free(kind);
+    free(src);
+    return rc;
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

@@ -49,6 +49,7 @@ def lib() -> C.CDLL:
         _lib.orc_view_angle.restype = C.c_float
         _lib.orc_num_threads.restype = C.c_int
         _lib.orc_grid_column.restype = C.c_int
+        _lib.orc_grid_pixel.restype = C.c_int
     return _lib
 
 
@@ -220,6 +221,21 @@ def grid_column(dNumU: int, dSize_mm: float, strip_um: int, inter_um: int, h_mm:
     out = np.empty(dNumU, np.float32)
     rc = lib().orc_grid_column(C.c_int64(dNumU), C.c_float(dSize_mm), strip_um, inter_um, C.c_float(h_mm),
                                C.c_float(FD_mm), C.c_float(mu_strip_mm), C.c_float(mu_inter_mm), _p(out))
+    if rc != 0:
+        raise ValueError("grid parameters out of range")
+    return out
+
+
+def grid_pixel(dNumU: int, dNumV: int, dSize_mm: float, strip_um: int, inter_um: int, h_mm: float, FD_mm: float,
+               mu_strip_mm, mu_inter_mm, rows=None) -> np.ndarray:
+    """Per-pixel, per-energy grid transmission [E][len(rows)][dNumU] in FP64
+    for the detector rows listed (all rows when None)."""
+    ms, mi = _f32(np.atleast_1d(mu_strip_mm)), _f32(np.atleast_1d(mu_inter_mm))
+    rows = np.arange(dNumV, dtype=np.int64) if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+    out = np.empty((len(ms), len(rows), dNumU), np.float64)
+    rc = lib().orc_grid_pixel(C.c_int64(dNumU), C.c_int64(dNumV), C.c_float(dSize_mm), strip_um, inter_um,
+                              C.c_float(h_mm), C.c_float(FD_mm), len(ms), _p(ms), _p(mi), C.c_int64(len(rows)),
+                              _p(rows), _p(out))
     if rc != 0:
         raise ValueError("grid parameters out of range")
     return out

@@ -146,6 +146,23 @@ def test_grid_column_parity_cases_mean_open_fraction(U, dsize, inter):
     assert np.max(np.abs(g - g[::-1])) < 0.02
 
 
+@pytest.mark.parametrize("U,dsize,strip,inter", [(64, 0.2, 50, 200), (64, 0.2, 49, 201), (63, 0.201, 50, 200),
+                                                 (63, 0.201, 30, 201), (40, 0.8, 50, 200)])
+def test_grid_pixel_central_row_is_the_column_model(U, dsize, strip, inter):
+    """The FP64 incidence-angle grid at y = 0 (the central row of an odd
+    detector) is the reference's column model (FP32 as the reference computes
+    it); rows off the centre transmit less, symmetrically about it."""
+    ms = np.array([30.0, 6.0, 2.0], np.float32)
+    mi = np.array([0.05, 0.01, 0.002], np.float32)
+    V = 9
+    g = O.grid_pixel(U, V, dsize, strip, inter, 2.0, 1500.0, ms, mi)
+    for e in range(3):
+        col = O.grid_column(U, dsize, strip, inter, 2.0, 1500.0, float(ms[e]), float(mi[e]))
+        assert np.max(np.abs(g[e, V // 2] - col) / col) < 3e-6
+    assert np.all(g[:, 0] < g[:, 1]) and np.all(g[:, 1] < g[:, V // 2])
+    np.testing.assert_allclose(g[:, 0], g[:, V - 1], rtol=1e-14)
+
+
 def test_finalize_floor_and_log():
     I = np.array([[[10.7, 0.4]]], np.float32)
     I0 = np.array([[20.0, 5.0]], np.float32)
