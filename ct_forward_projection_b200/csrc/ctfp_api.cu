@@ -41,6 +41,10 @@ struct ctfp_plan {
     int sampler = SAMPLER_LAYERED;
     cudaArray_t larr[kMaxM] = {};
     cudaTextureObject_t ltex[kMaxM] = {};
+    // axis sampler: copies layered along x and along y, written through surfaces
+    cudaArray_t xarr[kMaxM] = {}, yarr[kMaxM] = {};
+    cudaTextureObject_t xtex[kMaxM] = {}, ytex[kMaxM] = {};
+    cudaSurfaceObject_t xsurf[kMaxM] = {}, ysurf[kMaxM] = {};
     LaunchShape shape{};
     unsigned long long* d_count = nullptr;
     // empty-space skipping (off by default): brick occupancy, rebuilt from the
@@ -221,9 +225,57 @@ ctfp_status make_layered(ctfp_plan* p)
     return CTFP_OK;
 }
 
+// Layered array (width x height texels, `layers` layers) with a point-filter,
+// border-addressed texture object and a surface object for writing it.
+ctfp_status make_layered_rw(size_t width, size_t height, size_t layers, cudaArray_t& arr, cudaTextureObject_t& tex,
+                            cudaSurfaceObject_t& surf)
+{
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    CTFP_CUDA(cudaMalloc3DArray(&arr, &cd, make_cudaExtent(width, height, layers),
+                                cudaArrayLayered | cudaArraySurfaceLoadStore));
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    CTFP_CUDA(cudaCreateTextureObject(&tex, &rd, &td, nullptr));
+    CTFP_CUDA(cudaCreateSurfaceObject(&surf, &rd));
+    return CTFP_OK;
+}
+
+// The axis sampler's two copies per material: layered along x (texels
+// (y, z), a layer per x) and along y (texels (x, z), a layer per y).
+ctfp_status make_axis(ctfp_plan* p)
+{
+    const size_t nx = (size_t)p->geom.pNumX, ny = (size_t)p->geom.pNumY, nz = (size_t)p->geom.pNumZ;
+    for (int m = 0; m < p->M; m++) {
+        if (p->xarr[m]) continue;
+        ctfp_status st = make_layered_rw(ny, nz, nx, p->xarr[m], p->xtex[m], p->xsurf[m]);
+        if (st == CTFP_OK) st = make_layered_rw(nx, nz, ny, p->yarr[m], p->ytex[m], p->ysurf[m]);
+        if (st != CTFP_OK) return st;
+    }
+    return CTFP_OK;
+}
+
+bool axis_fits(const ctfp_geometry& g) { return g.pNumX <= 2048 && g.pNumY <= 2048 && g.pNumZ <= 32768; }
+
 void free_textures(ctfp_plan* p)
 {
     for (int m = 0; m < kMaxM; m++) {
+        if (p->xsurf[m]) cudaDestroySurfaceObject(p->xsurf[m]);
+        if (p->ysurf[m]) cudaDestroySurfaceObject(p->ysurf[m]);
+        if (p->xtex[m]) cudaDestroyTextureObject(p->xtex[m]);
+        if (p->ytex[m]) cudaDestroyTextureObject(p->ytex[m]);
+        if (p->xarr[m]) cudaFreeArray(p->xarr[m]);
+        if (p->yarr[m]) cudaFreeArray(p->yarr[m]);
+        p->xsurf[m] = p->ysurf[m] = 0;
+        p->xtex[m] = p->ytex[m] = 0;
+        p->xarr[m] = p->yarr[m] = nullptr;
         if (p->tex[m]) cudaDestroyTextureObject(p->tex[m]);
         if (p->arr[m]) cudaFreeArray(p->arr[m]);
         if (p->ltex[m]) cudaDestroyTextureObject(p->ltex[m]);
@@ -236,12 +288,19 @@ void free_textures(ctfp_plan* p)
 }
 
 bool uses_layered(const ctfp_plan* p) { return p->interp != INTERP_TEXTURE && p->sampler == SAMPLER_LAYERED; }
+bool uses_axis(const ctfp_plan* p) { return p->interp != INTERP_TEXTURE && p->sampler == SAMPLER_AXIS; }
 
 // Refreshes the plan's arrays (3D for TEXTURE, layered for the layered
 // sampler) from the caller's linear volumes; no-op for the global sampler.
 ctfp_status upload_textures(ctfp_plan* p, const float* const* volumes, cudaStream_t st)
 {
     const bool tex3d = p->interp == INTERP_TEXTURE;
+    if (uses_axis(p)) {
+        for (int m = 0; m < p->M; m++)
+            CTFP_CUDA(launch_axis_fill(volumes[m], (int)p->geom.pNumX, (int)p->geom.pNumY, (int)p->geom.pNumZ,
+                                       p->xsurf[m], p->ysurf[m], st));
+        return CTFP_OK;
+    }
     if (!tex3d && !uses_layered(p)) return CTFP_OK;
     for (int m = 0; m < p->M; m++) {
         cudaMemcpy3DParms cp;
@@ -279,6 +338,8 @@ MarchParams base_params(const ctfp_plan* p)
     for (int m = 0; m < kMaxM; m++) {
         prm.tex[m] = p->tex[m];
         prm.ltex[m] = p->ltex[m];
+        prm.xtex[m] = p->xtex[m];
+        prm.ytex[m] = p->ytex[m];
     }
     if (p->skip_empty && p->d_occ) {
         prm.occ = p->d_occ;
@@ -368,6 +429,10 @@ ctfp_status ctfp_plan_check_status(ctfp_plan* p, uint32_t* flags)
     CTFP_CUDA(cudaMemcpy(&v, p->d_status, sizeof(v), cudaMemcpyDeviceToHost));
     CTFP_CUDA(cudaMemset(p->d_status, 0, sizeof(v)));
     if (flags) *flags = v;
+    if (v & kCtfpStatusExitWaitTimeout)
+        return fail(CTFP_CUDA_ERROR,
+                    "a TMA-staged brick load was still in flight when its CTA exited: outputs since the last check "
+                    "and the shared memory of CTAs resident with it may be corrupt");
     if (v & kCtfpStatusWaitTimeout)
         return fail(CTFP_TIMEOUT, "a TMA-staged brick wait ran out; those samples were read from the volume");
     return CTFP_OK;
@@ -516,19 +581,24 @@ ctfp_status ctfp_plan_set_interp(ctfp_plan* p, int32_t interp)
     }
     p->interp = interp;
     if (uses_layered(p)) return make_layered(p);
+    if (uses_axis(p)) return make_axis(p);
     return CTFP_OK;
 }
 
 ctfp_status ctfp_plan_set_sampler(ctfp_plan* p, int32_t sampler)
 {
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
-    if (sampler != CTFP_SAMPLER_GLOBAL && sampler != CTFP_SAMPLER_LAYERED && sampler != CTFP_SAMPLER_BRICK)
+    if (sampler != CTFP_SAMPLER_GLOBAL && sampler != CTFP_SAMPLER_LAYERED && sampler != CTFP_SAMPLER_BRICK &&
+        sampler != CTFP_SAMPLER_AXIS)
         return fail(CTFP_INVALID_ARG, "unknown sampler");
     if (sampler == CTFP_SAMPLER_LAYERED && p->geom.pNumZ > 2048)
         return fail(CTFP_UNSUPPORTED, "layered sampler holds at most 2048 z slices");
+    if (sampler == CTFP_SAMPLER_AXIS && !axis_fits(p->geom))
+        return fail(CTFP_UNSUPPORTED, "axis sampler needs pNumX, pNumY <= 2048 and pNumZ <= 32768");
     DeviceScope ds(p->device);
     p->sampler = sampler;
     if (uses_layered(p)) return make_layered(p);
+    if (uses_axis(p)) return make_axis(p);
     return CTFP_OK;
 }
 

@@ -11,6 +11,8 @@ struct MarchParams {
     const float* vol[kMaxM];          // material densities [nz][ny][nx]
     cudaTextureObject_t tex[kMaxM];   // same volumes as 3D textures (TEXTURE mode)
     cudaTextureObject_t ltex[kMaxM];  // same volumes as layered 2D textures (SAMPLER_LAYERED)
+    cudaTextureObject_t xtex[kMaxM];  // SAMPLER_AXIS: layered along x (layer x, texel (y, z))
+    cudaTextureObject_t ytex[kMaxM];  // SAMPLER_AXIS: layered along y (layer y, texel (x, z))
     float* L;                         // [P][V][U][M] path integrals (out, may be null)
     const float* Lin;                 // [P][V][U][M] path integrals (in, epilogue/adjoint)
     float* I;                         // [P][V][U] (may be null)
@@ -32,8 +34,13 @@ struct MarchParams {
     int wait_limit;                   // polls of a TMA completion before a CTA gives up on staging
 };
 
-// Bits of the plan's device status word (ctfp_plan_check_status).
+// Bits of the plan's device status word (ctfp_plan_check_status; the same
+// values as CTFP_STATUS_* in ctfp.h).  WaitTimeout: a CTA gave up waiting for
+// a TMA load and read the volume instead (outputs correct).  ExitWaitTimeout:
+// the CTA's bounded wait at exit for that load ran out as well, so the copy may
+// have landed in shared memory another CTA owned (outputs not trusted).
 constexpr unsigned kCtfpStatusWaitTimeout = 1u;
+constexpr unsigned kCtfpStatusExitWaitTimeout = 2u;
 
 // Bricks of kOccShift^2 voxels per axis for empty-space skipping.  Brick
 // (bx, by, bz) is marked when any material has a non-zero voxel in
@@ -70,6 +77,11 @@ cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, c
 // of views view0.. (interp selects exact or texture-unit bilinear weights).
 cudaError_t launch_shift_views(const float* in, float* out, const GeomParams& g, int M, int interp, int view0,
                                int n_views, cudaStream_t st);
+// SAMPLER_AXIS: writes one volume [nz][ny][nx] into its x-layered copy
+// (surface xs: layer x, texel (y, z)) and its y-layered copy (ys: layer y,
+// texel (x, z)).
+cudaError_t launch_axis_fill(const float* vol, int nx, int ny, int nz, cudaSurfaceObject_t xs, cudaSurfaceObject_t ys,
+                             cudaStream_t st);
 // Fills occ [occ_dim(nz)][occ_dim(ny)][occ_dim(nx)] from the M volumes
 // (vol: host array of M device pointers; occ is zeroed first).
 cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st);

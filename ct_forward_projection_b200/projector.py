@@ -140,10 +140,12 @@ class Projector:
         self.interp = interp
 
     def set_sampler(self, sampler: str) -> None:
-        """'global' (linear volumes through L1), 'layered' (texture gathers) or
-        'brick' (per-bundle voxel boxes in shared memory)."""
+        """'global' (linear volumes through L1), 'layered' (texture gathers
+        from z-layered copies), 'axis' (gathers from copies layered along the
+        view's major in-plane axis, reused across samples) or 'brick'
+        (per-bundle voxel boxes in shared memory)."""
         call("ctfp_plan_set_sampler", self._h, {"global": capi.SAMPLER_GLOBAL, "layered": capi.SAMPLER_LAYERED,
-                                                 "brick": capi.SAMPLER_BRICK}[sampler])
+                                                 "brick": capi.SAMPLER_BRICK, "axis": capi.SAMPLER_AXIS}[sampler])
 
     def set_focal_spot(self, offset_u=None, offset_v=None) -> None:
         """Per-view focal-spot offsets in mm (ctfp_plan_set_focal_spot); None clears."""
@@ -162,7 +164,9 @@ class Projector:
     def check_status(self, raise_on_timeout: bool = False) -> int:
         """ctfp_plan_check_status: waits for the device, returns and clears
         the plan's status bits (1: a TMA-staged brick wait ran out; outputs
-        stay correct).  raise_on_timeout raises CtfpError(CTFP_TIMEOUT) then."""
+        stay correct).  raise_on_timeout raises CtfpError(CTFP_TIMEOUT) then.
+        Bit 2 (the wait at a CTA's exit ran out too: outputs not trusted)
+        always raises CtfpError(CTFP_CUDA_ERROR)."""
         flags = C.c_uint32()
         st = lib().ctfp_plan_check_status(self._h, C.byref(flags))
         if st == capi.CTFP_TIMEOUT and not raise_on_timeout:

@@ -95,7 +95,17 @@ typedef enum ctfp_sampler {
      * tensor load per material (cp.async.bulk.tensor) when pNumX is a multiple
      * of 4 and every volume starts on a 16-byte boundary, else plain loads;
      * CTFP_BRICK_STAGING=loads forces plain loads. */
-    CTFP_SAMPLER_BRICK = 3
+    CTFP_SAMPLER_BRICK = 3,
+    /* plan-owned layered 2D textures along the two in-plane axes: one copy per
+     * material layered along x (a layer per x index, texels (y, z)) and one
+     * layered along y.  Each view marches the copy layered along the axis its
+     * central ray runs closest to, so consecutive samples of a ray mostly keep
+     * their 2x2 in-layer footprint or move it one layer on; the gathers a ray
+     * already holds are kept in registers and only the missing layers are
+     * fetched (on poly_grid_256 about a third of the two gathers per sample of
+     * CTFP_SAMPLER_LAYERED).  Results are bitwise those of the layered sampler.
+     * Needs pNumX, pNumY <= 2048 and pNumZ <= 32768. */
+    CTFP_SAMPLER_AXIS = 4
 } ctfp_sampler;
 
 /* Grid transmission table layout for ctfp_set_spectral_tables. */
@@ -146,12 +156,22 @@ ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t 
  * sample.  No counterpart in the reference. */
 ctfp_status ctfp_plan_set_skip_empty(ctfp_plan* plan, int32_t enable);
 
+/* Bits of the plan's status word (ctfp_plan_check_status). */
+#define CTFP_STATUS_WAIT_TIMEOUT 1u      /* a staging wait ran out; outputs still correct */
+#define CTFP_STATUS_EXIT_WAIT_TIMEOUT 2u /* the wait at CTA exit ran out too; outputs not trusted */
+
 /* Waits for the device, then reads and clears the plan's status word: flags
  * receives its bits (may be NULL).  Returns CTFP_TIMEOUT when a kernel of the
  * plan gave up a bounded wait since the last check: a CTA of the TMA-staged
  * brick sampler whose tensor load did not complete within CTFP_WAIT_LIMIT
  * polls (default 65536) read those samples from the volume instead and stopped
- * staging, so its outputs are still correct.  No counterpart in the reference. */
+ * staging, so its outputs are still correct (CTFP_STATUS_WAIT_TIMEOUT).
+ * Returns CTFP_CUDA_ERROR when such a CTA's second bounded wait, before it
+ * exits, also ran out (CTFP_STATUS_EXIT_WAIT_TIMEOUT): the abandoned copy may
+ * have landed in shared memory that another CTA then owned, so the plan's
+ * outputs since the last check are not to be trusted.  No counterpart in the
+ * reference, whose launchers printed CUDA errors and carried on
+ * (Source/CUDAFun/CBCTPolyProjGPU.cu:55-61). */
 ctfp_status ctfp_plan_check_status(ctfp_plan* plan, uint32_t* flags);
 
 /* Focal spot (CBCTSinMatPolyForwardProj{Grid,NoGrid}::computePolyForwProjFoSp,
@@ -366,9 +386,15 @@ ctfp_status ctfp_backward_views(ctfp_plan* plan, const float* L_ckpt, const floa
  * interp must be CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU (the hardware
  * texture needs a cudaArray).  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls on a device share the array and it keeps the last call's
- * contents: calls whose work overlaps on the GPU (different streams or threads)
- * race on it and must be serialised by the caller. */
+ * capture.  That address is cached per device index for the life of the
+ * process: after the caller resets a device (cudaDeviceReset) the cached address
+ * no longer names the array, so a process that resets a device must not call
+ * this entry point on it again.  All calls on a device share the array and it
+ * keeps the last call's contents: calls whose work overlaps on the GPU
+ * (different streams or threads) race on it and must be serialised by the
+ * caller.  Speed: it reads each sample's 8 corners with plain loads from the
+ * caller's volumes (no plan-owned texture copies), about 3.6x the time of
+ * ctfp_forward's texture gathers on the 256^3 two-material grid workload. */
 #define CTFP_NOALLOC_MAX_VIEWS 8192
 #define CTFP_NOALLOC_SCRATCH_BYTES (200 * 1024)
 ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_materials, int32_t interp, int32_t n_energies,
