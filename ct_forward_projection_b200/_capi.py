@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOU
 
 INTERP_TRILINEAR, INTERP_TEXEMU, INTERP_TEXTURE = 0, 1, 2
 GRID_NONE, GRID_COLUMN, GRID_PIXEL = 0, 1, 2
-SAMPLER_GLOBAL, SAMPLER_LAYERED, SAMPLER_BRICK = 1, 2, 3
+SAMPLER_GLOBAL, SAMPLER_LAYERED, SAMPLER_BRICK, SAMPLER_AXIS = 1, 2, 3, 4
 MAX_MATERIALS = 4
 
 

@@ -18,9 +18,10 @@ namespace ctfp {
 
 enum { INTERP_TRILINEAR = 0, INTERP_TEXEMU = 1, INTERP_TEXTURE = 2 };
 // Where the software samplers (TRILINEAR, TEXEMU) read their 8 corners.
-enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2, SAMPLER_BRICK = 3 };
+// The values are those of ctfp_sampler (include/ctfp.h).
+enum { SAMPLER_GLOBAL = 1, SAMPLER_LAYERED = 2, SAMPLER_BRICK = 3, SAMPLER_AXIS = 4 };
 // Kernel-internal: the layered sampler with empty-space skipping.
-enum { SAMPLER_LAYERED_SKIP = 4 };
+enum { SAMPLER_LAYERED_SKIP = 16 };
 constexpr int kMaxM = 4;
 
 // Scalar geometry shared by every ray of one problem.
@@ -339,6 +340,19 @@ __device__ __forceinline__ float4 gather_layer(cudaTextureObject_t t, int layer,
     return r;
 }
 
+// gather_layer for gathers issued under a condition: a volatile asm is not
+// executed more often than the source says, so the compiler cannot turn the
+// conditional gather into an unconditional one plus a select (which would
+// spend the texture unit's time on every lane, the work a skipped gather saves).
+__device__ __forceinline__ float4 gather_layer_cond(cudaTextureObject_t t, int layer, float x, float y)
+{
+    float4 r;
+    asm volatile("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+                 : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+                 : "l"(t), "r"(layer), "f"(x), "f"(y), "f"(y));
+    return r;
+}
+
 // The 8 corners of M volumes held as layered 2D textures (one layer per z
 // slice): two gathers per material.  Layers outside [0, nz) read as 0 here,
 // since layer indices are clamped, not bordered, by the unit.
@@ -431,6 +445,21 @@ struct ScatterRun {
         }
     }
 };
+
+// exp(-a) and 1 - exp(-a), each to a few ulp relative, with one
+// transcendental: below a = 0.25 the absorbed fraction comes from expm1f, so
+// a thin ray's 1 - exp(-a) keeps its relative accuracy.  Every spectral
+// epilogue (plan forward, batch, no-allocation forward) uses this one function.
+__device__ __forceinline__ void transmit(float a, float& ex, float& om)
+{
+    if (a < 0.25f) {
+        om = -expm1f(-a);
+        ex = 1.0f - om;
+    } else {
+        ex = expf(-a);
+        om = 1.0f - ex;
+    }
+}
 
 // Compensated (Kahan) accumulation, FP32.
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x)

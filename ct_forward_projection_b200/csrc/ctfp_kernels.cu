@@ -90,18 +90,6 @@ __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, 
     for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
 }
 
-// exp(-a) and 1 - exp(-a), each to a few ulp relative, with one transcendental.
-__device__ __forceinline__ void transmit(float a, float& ex, float& om)
-{
-    if (a < 0.25f) {
-        om = -expm1f(-a);
-        ex = 1.0f - om;
-    } else {
-        ex = expf(-a);
-        om = 1.0f - ex;
-    }
-}
-
 // K2: I = sum_e W_e exp(-sum_m mu_em L_m), IAbs = sum_e W_e (1 - exp(...)).
 template <int M>
 __device__ __forceinline__ void spectral(const float* s_mu, int E, const float* __restrict__ W, int64_t pix,
@@ -183,6 +171,185 @@ __global__ void __launch_bounds__(256, MINB) k_forward(const MarchParams prm)
             spectral<M>(s_mu, prm.E, prm.W, pix, npix, L, I, A);
             if (prm.I) prm.I[ray] = I;
             if (prm.IAbs) prm.IAbs[ray] = A;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Axis sampler (SAMPLER_AXIS).  A view whose central ray runs mostly along x
+// reads the copies layered along x (layer = x index, texel (y, z)); any other
+// view reads the copies layered along y (layer = y, texel (x, z)).  A sample's
+// footprint is then two 2x2 gathers, layer Lc ("lo") and Lc + 1 ("hi"), at the
+// in-layer base (a, b).  Consecutive samples lie half a voxel apart, mostly
+// along the layer axis, so a sample usually has the previous sample's
+// footprint or the same in-layer base one layer on: each ray keeps its last two
+// gathers per material in registers and fetches only what it does not hold --
+// nothing, one layer (the other one moves over), or both when the in-layer
+// base changed.  The texture unit spends its time per active quad of 4 lanes,
+// so the lane layout (k_forward_axis) puts each quad on 4 adjacent detector
+// rows of one column: their rays cross layer and in-layer cell boundaries at
+// nearly the same samples and skip their gathers together.  Values, weights
+// and the order of the sums are the layered sampler's, so the results are
+// bitwise the same.
+
+// The 8 corners (k = dz*4 + dy*2 + dx) from the lo / hi gathers of one
+// material.  Gather order (tld4): x = (a, b+1), y = (a+1, b+1), z = (a+1, b),
+// w = (a, b), (a, b) the in-layer texel coordinates.
+template <int AX>
+__device__ __forceinline__ void axis_corners(const float4& lo, const float4& hi, float* v)
+{
+    if (AX == 0) {  // layer x, texel (y, z)
+        v[0] = lo.w; v[1] = hi.w; v[2] = lo.z; v[3] = hi.z;
+        v[4] = lo.x; v[5] = hi.x; v[6] = lo.y; v[7] = hi.y;
+    } else {  // layer y, texel (x, z)
+        v[0] = lo.w; v[1] = lo.z; v[2] = hi.w; v[3] = hi.z;
+        v[4] = lo.x; v[5] = lo.y; v[6] = hi.x; v[7] = hi.y;
+    }
+}
+
+// L_m for one ray with the axis sampler (AX 0: layered along x, 1: along y).
+template <int M, int MODE, int AX, bool SKIP>
+__device__ __forceinline__ void march_ray_axis(const MarchParams& prm, int p, int v, int u, float* L)
+{
+    const RaySeg s = ray_segment(prm.g, p, v, u);
+    RayRef32 r;
+    if (MODE != INTERP_TRILINEAR) r = ray_ref32(prm.g, p, v, u);
+    const cudaTextureObject_t* tx = AX == 0 ? prm.xtex : prm.ytex;
+    const int nl = AX == 0 ? prm.g.nx : prm.g.ny;
+    float acc[M], cmp[M];
+    float4 lo[M], hi[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        acc[m] = 0.f;
+        cmp[m] = 0.f;
+        lo[m] = hi[m] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // the held footprint: layer of lo and in-layer base; the sentinel layer
+    // matches no sample's (samples have footprint bases >= -2)
+    int cl = -1000000000, ca = 0, cb = 0;
+#pragma unroll 2
+    for (int i = s.i0; i < s.i1; i++) {
+        Corner c;
+        if (MODE == INTERP_TRILINEAR) {
+            const double t = (double)i;
+            c = corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
+        } else {
+            c = corner_tex(ref32_coords(prm.g, r, i));
+        }
+        if (SKIP && !footprint_occupied(prm, c)) continue;
+        const int lc = AX == 0 ? c.ix : c.iy;
+        const int a = AX == 0 ? c.iy : c.ix;
+        const int b = c.iz;
+        const bool base = (a == ca) & (b == cb);
+        const bool same = base & (lc == cl);
+        const bool up = base & (lc == cl + 1);  // one layer on in +axis: old hi is the new lo
+        const bool dn = base & (lc == cl - 1);  // one layer on in -axis: old lo is the new hi
+        if (up) {
+#pragma unroll
+            for (int m = 0; m < M; m++) lo[m] = hi[m];
+        }
+        if (dn) {
+#pragma unroll
+            for (int m = 0; m < M; m++) hi[m] = lo[m];
+        }
+        const float fa = (float)(a + 1), fb = (float)(b + 1);
+        if (!same && !up) {
+            // layers outside the volume read 0 (the unit clamps layer indices)
+            const bool ok = (unsigned)lc < (unsigned)nl;
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const float4 g4 = gather_layer_cond(tx[m], ok ? lc : 0, fa, fb);
+                lo[m] = ok ? g4 : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        if (!same && !dn) {
+            const bool ok = (unsigned)(lc + 1) < (unsigned)nl;
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const float4 g4 = gather_layer_cond(tx[m], ok ? lc + 1 : 0, fa, fb);
+                hi[m] = ok ? g4 : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        cl = lc;
+        ca = a;
+        cb = b;
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            float cv[8];
+            axis_corners<AX>(lo[m], hi[m], cv);
+            kahan_add(acc[m], cmp[m], interp8<MODE>(c, cv));
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
+}
+
+// Whether view p reads the x-layered copies: its central ray (direction
+// (cos th, -sin th) in the volume's x-y plane) advances at least as many x
+// voxels as y voxels per step.
+__device__ __forceinline__ bool axis_is_x(const GeomParams& g, int p)
+{
+    const double2 cs = g.trig[p];
+    return fabs(cs.x) * (double)g.pSizeY >= fabs(cs.y) * (double)g.pSizeX;
+}
+
+// K1+K2 with the axis sampler.  One-dimensional CTAs of tile_u * tile_v
+// threads (tile_v a multiple of 4) cover a tile_u x tile_v pixel tile: lane
+// quads run down 4 detector rows of one column, so a warp covers 8 columns x
+// 4 rows.  Grid: x = pixel tiles along u, y = along v, z = view groups.
+template <int M, int MODE, bool SKIP, bool SPECTRAL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_forward_axis(const MarchParams prm, int tile_u)
+{
+    extern __shared__ float s_mu[];
+    if (SPECTRAL) load_mu(s_mu, prm.mu, prm.E * M);
+    const int tid = threadIdx.x;
+    const int q = tid >> 2;
+    const int tile_v = (int)blockDim.x / tile_u;
+    const int u = blockIdx.x * tile_u + q % tile_u;
+    const int v = blockIdx.y * tile_v + 4 * (q / tile_u) + (tid & 3);
+    if (u >= prm.g.U || v >= prm.g.V) return;
+    const int64_t npix = (int64_t)prm.g.U * prm.g.V;
+    const int64_t pix = (int64_t)v * prm.g.U + u;
+    const int pend = prm.view0 + prm.n_views;
+    for (int k = 0; k < prm.views_per_cta; k++) {
+        const int p = prm.view0 + blockIdx.z * prm.views_per_cta + k;
+        if (p >= pend) break;
+        float L[M];
+        if (axis_is_x(prm.g, p)) march_ray_axis<M, MODE, 0, SKIP>(prm, p, v, u, L);
+        else march_ray_axis<M, MODE, 1, SKIP>(prm, p, v, u, L);
+        const int64_t ray = (int64_t)(p - prm.out_view0) * npix + pix;
+        if (prm.L) store_L<M>(prm.L, ray, L);
+        if (SPECTRAL) {
+            float I, A;
+            spectral<M>(s_mu, prm.E, prm.W, pix, npix, L, I, A);
+            if (prm.I) prm.I[ray] = I;
+            if (prm.IAbs) prm.IAbs[ray] = A;
+        }
+    }
+}
+
+// The x- and y-layered copies of one volume, through a 32 x 32 (x, y) tile
+// of one z slice in shared memory so that both copies are written along their
+// texel rows.  Block (32, 8); grid (ceil(nx / 32), ceil(ny / 32), nz).
+__global__ void __launch_bounds__(256) k_axis_fill(const float* __restrict__ vol, int nx, int ny,
+                                                   cudaSurfaceObject_t xs, cudaSurfaceObject_t ys)
+{
+    __shared__ float t[32][33];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, z = blockIdx.z;
+    const int tx = threadIdx.x;
+    for (int ty = threadIdx.y; ty < 32; ty += 8) {
+        const int x = x0 + tx, y = y0 + ty;
+        t[ty][tx] = (x < nx && y < ny) ? __ldg(vol + ((size_t)z * ny + y) * nx + x) : 0.f;
+    }
+    __syncthreads();
+    for (int ty = threadIdx.y; ty < 32; ty += 8) {
+        {
+            const int x = x0 + tx, y = y0 + ty;  // y-layered: layer y, texel (x, z)
+            if (x < nx && y < ny) surf2DLayeredwrite(t[ty][tx], ys, x * (int)sizeof(float), z, y);
+        }
+        {
+            const int y = y0 + tx, x = x0 + ty;  // x-layered: layer x, texel (y, z)
+            if (x < nx && y < ny) surf2DLayeredwrite(t[tx][ty], xs, y * (int)sizeof(float), z, x);
         }
     }
 }
@@ -529,7 +696,8 @@ __global__ void __launch_bounds__(kBU * kBV, MINB) k_forward_brick(const MarchPa
 // all later ones from the volume (same results), ors kCtfpStatusWaitTimeout
 // into the plan's status word, and before exiting waits, again bounded, for
 // the load still in flight so that it cannot land in shared memory the CTA no
-// longer owns.
+// longer owns; when that exit wait runs out as well, it ors
+// kCtfpStatusExitWaitTimeout, an error (outputs not trusted).
 constexpr int kTX = 20;
 constexpr int kTRow = kTX, kTSlice = kTX * kBY;
 constexpr int kTBoxFloats = kTSlice * kBZ;  // 6400 floats = 25600 bytes, a multiple of 128
@@ -704,8 +872,13 @@ __global__ void __launch_bounds__(kBU * kBV, MINB)
         }
     }
     // a load given up on may still be writing the box: wait for it (bounded)
-    // before the CTA's shared memory is released
-    if (in_flight) mbar_wait_bounded(&s_bar, phase, kExitPolls);
+    // before the CTA's shared memory is released; if that wait runs out too,
+    // the copy may land in shared memory another CTA then owns, which the
+    // plan's status word reports as an error (kCtfpStatusExitWaitTimeout)
+    if (in_flight) {
+        const bool landed = mbar_wait_bounded(&s_bar, phase, kExitPolls);
+        if (!landed && tid == 0 && prm.status) atomicOr(prm.status, kCtfpStatusExitWaitTimeout);
+    }
 }
 
 // The dynamic shared-memory opt-in is per device and per kernel; plans on
@@ -840,6 +1013,40 @@ cudaError_t fwd_dispatch_mode(const MarchParams& prm, int interp, int sampler, b
     return cudaErrorInvalidValue;
 }
 
+template <int M, int MODE, bool SKIP, int MINB>
+cudaError_t axis_launch(const MarchParams& prm, bool spec, int tile_u, dim3 grid, dim3 block, size_t smem,
+                        cudaStream_t st)
+{
+    if (spec) k_forward_axis<M, MODE, SKIP, true, MINB><<<grid, block, smem, st>>>(prm, tile_u);
+    else k_forward_axis<M, MODE, SKIP, false, MINB><<<grid, block, 0, st>>>(prm, tile_u);
+    return cudaGetLastError();
+}
+
+template <int M, int MODE, bool SKIP>
+cudaError_t axis_dispatch_minb(const MarchParams& prm, bool spec, int minb, int tile_u, dim3 grid, dim3 block,
+                               size_t smem, cudaStream_t st)
+{
+    switch (minb) {
+        case 3: return axis_launch<M, MODE, SKIP, 3>(prm, spec, tile_u, grid, block, smem, st);
+        case 4: return axis_launch<M, MODE, SKIP, 4>(prm, spec, tile_u, grid, block, smem, st);
+        default: return axis_launch<M, MODE, SKIP, 2>(prm, spec, tile_u, grid, block, smem, st);
+    }
+}
+
+template <int M>
+cudaError_t axis_dispatch(const MarchParams& prm, int interp, bool spec, int minb, int tile_u, dim3 grid,
+                          dim3 block, size_t smem, cudaStream_t st)
+{
+    const bool skip = prm.occ != nullptr;
+    if (interp == INTERP_TRILINEAR)
+        return skip ? axis_dispatch_minb<M, INTERP_TRILINEAR, true>(prm, spec, minb, tile_u, grid, block, smem, st)
+                    : axis_dispatch_minb<M, INTERP_TRILINEAR, false>(prm, spec, minb, tile_u, grid, block, smem, st);
+    if (interp == INTERP_TEXEMU)
+        return skip ? axis_dispatch_minb<M, INTERP_TEXEMU, true>(prm, spec, minb, tile_u, grid, block, smem, st)
+                    : axis_dispatch_minb<M, INTERP_TEXEMU, false>(prm, spec, minb, tile_u, grid, block, smem, st);
+    return cudaErrorInvalidValue;
+}
+
 template <int M>
 cudaError_t bwd_dispatch(const MarchParams& prm, int interp, bool from_gL, dim3 grid, dim3 block, size_t smem,
                          cudaStream_t st)
@@ -886,6 +1093,25 @@ cudaError_t launch_forward_once(const MarchParams& prm, int M, int interp, int s
         }
         return cudaErrorInvalidValue;
     }
+    if (sampler == SAMPLER_AXIS && interp != INTERP_TEXTURE) {
+        // lane quads run down 4 detector rows: tiles whose height is not a
+        // multiple of 4 use 16 x 16
+        LaunchShape as = ls;
+        if (as.tile_v % 4 != 0 || as.tile_u * as.tile_v > 256 || (as.tile_u * as.tile_v) % 32 != 0) {
+            as.tile_u = 16;
+            as.tile_v = 16;
+        }
+        const dim3 block(as.tile_u * as.tile_v), grid = march_grid(prm, as);
+        const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
+        if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
+        switch (M) {
+            case 1: return axis_dispatch<1>(prm, interp, do_spectral, as.min_ctas, as.tile_u, grid, block, smem, st);
+            case 2: return axis_dispatch<2>(prm, interp, do_spectral, as.min_ctas, as.tile_u, grid, block, smem, st);
+            case 3: return axis_dispatch<3>(prm, interp, do_spectral, as.min_ctas, as.tile_u, grid, block, smem, st);
+            case 4: return axis_dispatch<4>(prm, interp, do_spectral, as.min_ctas, as.tile_u, grid, block, smem, st);
+        }
+        return cudaErrorInvalidValue;
+    }
     const dim3 block(ls.tile_u, ls.tile_v), grid = march_grid(prm, ls);
     const size_t smem = do_spectral ? sizeof(float) * (size_t)prm.E * M : 0;
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
@@ -915,6 +1141,15 @@ cudaError_t launch_forward(const MarchParams& prm_in, int M, int interp, int sam
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_axis_fill(const float* vol, int nx, int ny, int nz, cudaSurfaceObject_t xs, cudaSurfaceObject_t ys,
+                             cudaStream_t st)
+{
+    const dim3 grid((nx + 31) / 32, (ny + 31) / 32, nz);
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return cudaSuccess;
+    k_axis_fill<<<grid, dim3(32, 8), 0, st>>>(vol, nx, ny, xs, ys);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st)

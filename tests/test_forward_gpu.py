@@ -48,7 +48,7 @@ GEOMS = [
 ]
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick", "axis"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 3, 4])
 def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
@@ -61,7 +61,7 @@ def test_line_integrals_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
     assert rel_err_scaled(L, Lref) < RTOL_TRI
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick", "axis"])
 @pytest.mark.parametrize("gi", range(len(GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 4])
 def test_forward_trilinear_vs_oracle(cuda_ok, gi, M, sampler):
@@ -89,7 +89,8 @@ ANISO = dict(pNumX=20, pNumY=16, pNumZ=10, pLengthX=20.0, pLengthY=12.0, pLength
 
 
 @pytest.mark.parametrize("mode,sampler", [("trilinear", "layered"), ("trilinear", "global"), ("trilinear", "brick"),
-                                          ("texemu", "layered"), ("texture", None)])
+                                          ("trilinear", "axis"), ("texemu", "layered"), ("texemu", "axis"),
+                                          ("texture", None)])
 def test_anisotropic_voxels_vs_oracle(cuda_ok, mode, sampler):
     d = dict(ANISO)
     M = 2
@@ -130,7 +131,7 @@ def test_forward_grid_layouts_and_no_response(cuda_ok, layout):
     assert rel_err(out["IAbsorb"].cpu(), ref["IAbsorb"]) < RTOL_TRI
 
 
-@pytest.mark.parametrize("sampler", ["layered", "global", "brick"])
+@pytest.mark.parametrize("sampler", ["layered", "global", "brick", "axis"])
 @pytest.mark.parametrize("M", [1, 2, 3])
 def test_forward_texemu_vs_oracle(cuda_ok, M, sampler):
     d = small_geometry(n=20, views=5, U=24, V=14)
@@ -490,3 +491,78 @@ def test_deep_volume_falls_back_to_global_sampler(cuda_ok):
             pr.set_sampler("layered")
         assert e.value.status == CTFP_UNSUPPORTED
     assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
+
+
+# geometries for the axis sampler: views all round the rotation (both copies,
+# rays marching up and down each axis), anisotropic voxels, the reversed
+# rotation, detector sizes that leave partial tiles and partial lane quads
+AXIS_GEOMS = [
+    dict(n=(26, 22, 18), views=37, U=21, V=14),
+    dict(n=16, views=24, U=33, V=9, rot=-1),
+    dict(n=(9, 23, 14), views=19, U=8, V=41),
+]
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("gi", range(len(AXIS_GEOMS)))
+@pytest.mark.parametrize("M", [1, 2, 3, 4])
+def test_axis_sampler_equals_layered(cuda_ok, mode, gi, M):
+    """The axis sampler reads the same voxel values with the same weights in
+    the same order as the layered sampler: outputs are bitwise equal."""
+    d = small_geometry(**AXIS_GEOMS[gi])
+    vols = random_volumes(d, M, 500 + 10 * gi + M)
+    S, mu, G, D = spectral_setup(d, M, 7, 3 + gi)
+    with Projector(d, M, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_sampler("layered")
+        a = pr.forward(to_dev(vols), want_L=True)
+        pr.set_sampler("axis")
+        b = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    for k in ("L", "I", "IAbsorb", "I0"):
+        assert torch.equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+@pytest.mark.parametrize("shape", [(16, 16, 1, 3), (32, 8, 2, 4), (8, 32, 4, 2), (16, 4, 1, 3), (64, 2, 1, 3)])
+def test_axis_sampler_launch_shapes(cuda_ok, mode, shape):
+    """Every launch shape gives the same outputs (tiles whose height is not a
+    multiple of 4 run as 16 x 16)."""
+    d = small_geometry(n=(20, 24, 16), views=9, U=37, V=23)
+    vols = random_volumes(d, 2, 77)
+    S, mu, G, D = spectral_setup(d, 2, 5, 8)
+    with Projector(d, 2, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        a = pr.forward(to_dev(vols), want_L=True)
+        pr.set_sampler("axis")
+        pr.set_launch_shape(*shape)
+        b = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    assert torch.equal(a["L"], b["L"]) and torch.equal(a["I"], b["I"])
+
+
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+def test_axis_sampler_skip_empty(cuda_ok, mode):
+    d = small_geometry(n=(40, 36, 30), views=11, U=37, V=29)
+    vols = _sparse_volumes(d, 2, 91)
+    S, mu, G, D = spectral_setup(d, 2, 7, 3)
+    with Projector(d, 2, mode) as pr:
+        pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_sampler("axis")
+        full = pr.forward(to_dev(vols), want_L=True)
+        pr.set_skip_empty(True)
+        skip = pr.forward(to_dev(vols), want_L=True)
+        torch.cuda.synchronize()
+    for k in ("I", "IAbsorb"):
+        assert rel_err(skip[k].cpu().numpy(), full[k].cpu().numpy()) < 1e-6
+    assert rel_err_scaled(skip["L"].cpu().numpy(), full["L"].cpu().numpy()) < 1e-6
+
+
+def test_axis_sampler_limits(cuda_ok):
+    # the copies are layered along x and y: at most 2048 layers each
+    from ct_forward_projection_b200._capi import CtfpError, CTFP_UNSUPPORTED
+    d = small_geometry(n=(2050, 4, 3), views=2, U=7, V=5, length=20.0, pitch=2.0)
+    with Projector(d, 1, "trilinear") as pr:
+        with pytest.raises(CtfpError) as e:
+            pr.set_sampler("axis")
+        assert e.value.status == CTFP_UNSUPPORTED
