@@ -165,13 +165,7 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
         for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
         const float w = __ldg(it.W + (int64_t)e * npix + pix);
         float ex, om;
-        if (att < 0.25f) {
-            om = -expm1f(-att);
-            ex = 1.0f - om;
-        } else {
-            ex = expf(-att);
-            om = 1.0f - ex;
-        }
+        transmit(att, ex, om);
         const float Ie = w * ex;
         kahan_add(sI, cI, Ie);
         if (!ADJOINT) kahan_add(sA, cA, w * om);

@@ -117,13 +117,7 @@ __global__ void __launch_bounds__(256) k_forward_noalloc(const NoallocParams q)
         for (int m = 0; m < M; m++) att = fmaf(q.mu[e * M + m], L[m], att);
         const float w = weight_of(q, e, u, pix, npix);
         float ex, om;
-        if (att < 0.25f) {
-            om = -expm1f(-att);
-            ex = 1.0f - om;
-        } else {
-            ex = expf(-att);
-            om = 1.0f - ex;
-        }
+        transmit(att, ex, om);
         kahan_add(sI, cI, w * ex);
         kahan_add(sA, cA, w * om);
     }

@@ -116,3 +116,30 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                          capi.ptr_array([v.data_ptr()]), out.data_ptr(), out.data_ptr(), None,
                                          None)
     assert st == capi.CTFP_UNSUPPORTED
+
+
+@pytest.mark.parametrize("interp", [0, 1])
+def test_noalloc_without_grid_response_or_flat_field(interp):
+    """The optional inputs: no grid table (layout 0), no detector response
+    (D NULL) and no flat-field output (I0 NULL, its kernel skipped), with one
+    material and with four, against the plan forward on the same inputs."""
+    for k, (geo, M, layout, with_D) in enumerate([(dict(n=16, views=5, U=19, V=11), 1, 0, False),
+                                                  (dict(n=(14, 18, 12), views=6, U=15, V=13), 4, 2, False),
+                                                  (dict(n=12, views=3, U=9, V=21, rot=-1), 4, 0, True)]):
+        d = small_geometry(**geo)
+        vols = [torch.from_numpy(v).cuda() for v in random_volumes(d, M, 950 + k)]
+        S, mu, G, D = spectral_setup(d, M, 9, 60 + k, grid=layout != 0, det=with_D)
+        with Projector(d, M, "trilinear" if interp == 0 else "texemu") as pr:
+            pr.set_spectral_tables(S, mu, G, layout, D, 1000.0)
+            ref = pr.forward(vols)
+            torch.cuda.synchronize()
+        c = _prepare(d, vols, S, mu, G, D)
+        for _ in range(2):
+            capi.call("ctfp_forward_noalloc", C.byref(c["g"]), M, interp, len(c["S"]),
+                      c["S"].ctypes.data_as(C.c_void_p), c["mu"].ctypes.data_as(C.c_void_p),
+                      None if c["G"] is None else c["G"].data_ptr(), layout,
+                      None if c["D"] is None else c["D"].data_ptr(), C.c_float(1000.0), c["ptrs"],
+                      c["I"].data_ptr(), c["A"].data_ptr(), None, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            assert _rel(c["I"], ref["I"]) < RTOL
+            assert _rel(c["A"], ref["IAbsorb"]) < RTOL
