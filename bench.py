@@ -161,28 +161,42 @@ def _err_stats(x: np.ndarray) -> dict:
     return {"max": float(np.max(x)), "p99": float(np.percentile(x, 99))}
 
 
+def _ray_ids(rng, g, rows, n):
+    """n distinct seeded ray ids (view, row, column) whose detector row is one
+    of rows (every row when rows is None), sorted."""
+    P, V, U = int(g["projNum"]), int(g["dNumV"]), int(g["dNumU"])
+    rows = np.arange(V) if rows is None else np.asarray(rows)
+    n_sel = P * len(rows) * U
+    k = np.sort(rng.choice(n_sel, min(n, n_sel), replace=False))
+    p, rem = np.divmod(k, len(rows) * U)
+    r, u = np.divmod(rem, U)
+    return np.sort((p * V + rows[r]) * U + u).astype(np.int64)
+
+
 def cpu_baseline(w, gpu: dict, budget_s: float):
     """FP64 oracle over a seeded subset of rays on all host cores; also the
     error of the GPU result on those rays: per-ray relative error of I,
     IAbsorb and I0 (max and 99th percentile) and the absolute error of the
-    compat projection log(I0 / floor(I)) (CBCTForwardProj.cpp:376-387)."""
+    compat projection log(I0 / floor(I)) (CBCTForwardProj.cpp:376-387).
+    The rays lie on the detector rows whose oracle energy weights were built
+    (w._rows, oracle_weights)."""
     from oracle import oracle as O
-    from ct_forward_projection_b200.projector import Projector  # noqa: F401  (tables below)
     g = w.geometry
-    n_rays = w.n_rays
+    rows = getattr(w, "_rows", None)
     rng = np.random.RandomState(7)
     vols = [v.cpu().numpy() for v in w._vols]
     W = w._W
     mu = w.mu_table()
     # warm the thread pool, calibrate on a subset, then size the sample to the budget
-    n0 = min(8192, n_rays)
-    O.forward(g, vols, mu, W, O.TRILINEAR, np.sort(rng.choice(n_rays, min(512, n_rays), replace=False)))
-    ids = np.sort(rng.choice(n_rays, n0, replace=False))
+    n0 = min(8192, w.n_rays)
+    O.forward(g, vols, mu, W, O.TRILINEAR, _ray_ids(rng, g, rows, 512))
+    ids = _ray_ids(rng, g, rows, n0)
     t0 = time.perf_counter()
     O.forward(g, vols, mu, W, O.TRILINEAR, ids)
     dt = time.perf_counter() - t0
-    n = int(min(n_rays, max(n0, n0 * budget_s / max(dt, 1e-6))))
-    ids = np.sort(rng.choice(n_rays, n, replace=False))
+    n = int(max(len(ids), len(ids) * budget_s / max(dt, 1e-6)))
+    ids = _ray_ids(rng, g, rows, n)
+    n = len(ids)
     t0 = time.perf_counter()
     ref = O.forward(g, vols, mu, W, O.TRILINEAR, ids)
     dt = time.perf_counter() - t0
@@ -199,9 +213,13 @@ def cpu_baseline(w, gpu: dict, budget_s: float):
     acc["proj_abs"] = _err_stats(np.abs(proj_got - proj_ref))
     acc["proj_abs"]["note"] = "includes the floor to integer counts: I one count apart near an integer gives ~1/I"
     acc["rays"] = n
+    acc["tables"] = getattr(w, "_tables", "as given")
+    if rows is not None:
+        acc["detector_rows"] = [int(r) for r in rows]
+    where = "all detector rows" if rows is None else f"{len(rows)} seeded detector rows"
     cpu = {"value": n / dt, "unit": "rays/s", "cores": O.num_threads(), "kind": "port",
            "cpu_model": _cpu_model(),
-           "sample": f"{n} seeded random rays (seed 7) of the full workload, FP64 oracle, {dt:.1f} s"}
+           "sample": f"{n} seeded random rays (seed 7) on {where} of the full workload, FP64 oracle, {dt:.1f} s"}
     return cpu, acc
 
 
@@ -240,7 +258,7 @@ def reference_arm(args, w, ws, rank):
     vols = [v.cpu().numpy() for v in w._vols]
     n = 4096
     for s in range(args.warmup + args.steps):
-        ids = np.sort(rng.choice(w.n_rays, n, replace=False))
+        ids = _ray_ids(rng, g, getattr(w, "_rows", None), n)
         t0 = time.perf_counter()
         O.forward(g, vols, mu, w._W, O.TRILINEAR, ids)
         dt = time.perf_counter() - t0
@@ -271,7 +289,7 @@ def main():
     ap.add_argument("--shard", default="objects", choices=["objects", "views"],
                     help="N > 1: each rank projects its own object (weak scaling) or a slab of one "
                          "object's views (strong scaling; the adjoint sums gradients with all-reduce)")
-    ap.add_argument("--sampler", default="layered", choices=["layered", "global", "brick"],
+    ap.add_argument("--sampler", default="layered", choices=["layered", "global", "brick", "axis"],
                     help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
                     help="problems in the uneven batch leg (0 skips it)")
@@ -296,9 +314,9 @@ def main():
         w = physics.workload(args.workload)
         w._vols = physics.phantom(w, "cpu")
         if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ctfp_ref")):
-            # the oracle port stands in: its energy weights come from the
-            # library's table builders (the reference binary runs none of this)
-            w._W = _weights_from_tables(w, local)
+            # the oracle port stands in, with its own tables
+            w._rows = oracle_rows(w)
+            w._W, w._tables = oracle_weights(w, w._rows)
         line = reference_arm(args, w, ws, rank)
         if line is not None:
             print(json.dumps(line), flush=True)
@@ -481,7 +499,8 @@ def main():
     err = acc = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         w._vols = vols
-        w._W = _weights_from_tables(w, local)
+        w._rows = oracle_rows(w)
+        w._W, w._tables = oracle_weights(w, w._rows)
         gpu = {k: out[k].cpu().numpy() for k in ("I", "IAbsorb")}
         gpu["I0"] = pr.forward(vols, views=(0, 1))["I0"].cpu().numpy()  # view-independent; not in the timed step
         cpu, acc = cpu_baseline(w, gpu, args.cpu_budget)
@@ -654,8 +673,9 @@ def batch_leg(args, ws, rank, local, stream):
         rng = np.random.RandomState(3)
         for k in (0, len(wl) // 2, len(wl) - 1):
             w = wl[k]
-            W = _weights_from_tables(w, local)
-            ids = np.sort(rng.choice(w.n_rays, 1024, replace=False))
+            rows = oracle_rows(w, 4)
+            W, _ = oracle_weights(w, rows)
+            ids = _ray_ids(rng, w.geometry, rows, 1024)
             ref = O.forward(w.geometry, [x.cpu().numpy() for x in vols[k]], w.mu_table(), W, O.TRILINEAR, ids)
             got = b_outs[k]["I"].reshape(-1)[torch.from_numpy(ids).to(dev)].double().cpu().numpy()
             oerr = max(oerr, float(np.max(np.abs(got - ref["I"]) / np.abs(ref["I"]))))
@@ -678,26 +698,56 @@ def batch_leg(args, ws, rank, local, stream):
     }
 
 
-def _weights_from_tables(w, device):
-    """Energy weights W[e][v][u] in FP64 for the oracle, from the same device
-    tables the projector uses (grid, scintillator)."""
-    import torch
+def oracle_rows(w, n_rows: int = 16, seed: int = 5):
+    """The detector rows on which the oracle checks a workload with a per-pixel
+    grid table: the outermost, the two central and n_rows - 4 seeded rows
+    (None, meaning every row, for tables without a per-row dependence)."""
+    V = int(w.geometry["dNumV"])
+    if w.grid is None or w.grid_layout != 2 or V <= n_rows:
+        return None
+    rng = np.random.RandomState(seed)
+    rows = {0, V - 1, V // 2 - 1, V // 2}
+    while len(rows) < n_rows:
+        rows.add(int(rng.randint(0, V)))
+    return np.array(sorted(rows), np.int64)
 
-    from ct_forward_projection_b200.projector import build_det_response, build_grid_table, scintillator_thickness
+
+def oracle_weights(w, rows=None):
+    """Energy weights W[e][v][u] = I0Val * S_e * G_e * D_e in FP64 for the
+    oracle, built from the oracle's own tables and nothing of the library:
+    the grid by orc_grid_column (column layout) or orc_grid_pixel (per-pixel
+    incidence-angle layout, on the rows listed; other rows hold NaN so that a
+    ray there cannot pass unnoticed), the scintillator response by
+    orc_scint_thickness and orc_det_response.  Returns (W, description)."""
     from oracle import oracle as O
     g = w.geometry
     U, V = int(g["dNumU"]), int(g["dNumV"])
     E = len(w.energies)
-    G = None
+    W = np.full((E, V, U), w.I0Val, np.float64) * w.spectrum().astype(np.float64)[:, None, None]
+    built = ["spectrum"]
+    sel = np.arange(V) if rows is None else np.asarray(rows)
     if w.grid is not None:
         ms, mi = w.grid_mu()
-        G = build_grid_table(g, w.grid, ms, mi, w.grid_layout, device=device).cpu().numpy()
-    D = None
+        gs = w.grid
+        if w.grid_layout == 2:
+            G = O.grid_pixel(U, V, float(g["dSize"]), gs.strip_um, gs.inter_um, gs.h_mm, gs.FD_mm, ms, mi, sel)
+            built.append(f"grid orc_grid_pixel ({len(sel)} rows)")
+        else:
+            col = np.stack([O.grid_column(U, float(g["dSize"]), gs.strip_um, gs.inter_um, gs.h_mm, gs.FD_mm,
+                                          float(ms[e]), float(mi[e])) for e in range(E)]).astype(np.float64)
+            G = np.repeat(col[:, None, :], len(sel), axis=1)
+            built.append("grid orc_grid_column")
+        W[:, sel, :] *= G
     if w.scint_mm is not None:
-        t = scintillator_thickness(U * V, w.scint_mm, w.scint_err_mm)
-        D = build_det_response(w.scint_mu(), torch.from_numpy(t).to(f"cuda:{device}"), 1.0).cpu().numpy()
-        D = D.reshape(E, V, U)
-    return O.energy_weights(g, w.spectrum(), G, w.grid_layout if G is not None else 0, D, w.I0Val)
+        t = O.scint_thickness(U * V, w.scint_mm, w.scint_err_mm)
+        D = O.det_response(w.scint_mu(), t, 1.0).reshape(E, V, U).astype(np.float64)
+        W *= D
+        built.append("scintillator orc_scint_thickness + orc_det_response")
+    if rows is not None:
+        keep = np.zeros(V, bool)
+        keep[sel] = True
+        W[:, ~keep, :] = np.nan
+    return W, "oracle: " + ", ".join(built)
 
 
 if __name__ == "__main__":

@@ -20,7 +20,9 @@ REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(cd "$HERE/.." && pwd)
 OUT="$HERE/_ref"
-[ -d "$REF/Source" ] || { echo "reference sources not found at $REF" >&2; exit 0; }
+# without the sources (e.g. on a GPU box, which uses the binary built here)
+# there is nothing to build
+[ -d "$REF/Source" ] || { echo "reference sources not found at $REF; oracle/_ref not built" >&2; exit 0; }
 BIN="$OUT/ctfp_ref"
 # rebuild only when the recipe or the shims are newer than the binary
 if [ -x "$BIN" ] && [ "$BIN" -nt "$HERE/build_ref.sh" ] && [ "$BIN" -nt "$HERE/ref_shim/ref_compat.h" ] \

@@ -7,6 +7,7 @@ import sys
 import time
 
 import bench
+import numpy as np
 
 FAKE = """#!{python}
 import datetime, sys, time
@@ -100,3 +101,33 @@ def test_cpu_baseline_accuracy_figures():
         assert acc[k]["max"] < 1e-7 and acc[k]["p99"] <= acc[k]["max"]
     assert acc["proj_abs"]["max"] < 1e-3
     assert acc["rays"] == n
+
+
+def test_reference_arm_extrapolates_the_full_view_step(monkeypatch):
+    # the reference arm's runs alternate between two view counts; a line
+    # T(n) = F + n t through their wall times predicts the full-view step.
+    # A stand-in for the reference binary takes F = 5 s + 0.25 s per view.
+    import types
+
+    from ct_forward_projection_b200 import physics
+    from oracle import ref_runner
+    calls = []
+
+    def fake_run(case, timeout=600.0, keep_dir=None):
+        n = case["geometry"]["projNum"]
+        calls.append(n)
+        return {}, 5.0 + 0.25 * n, ""
+
+    monkeypatch.setattr(ref_runner, "run", fake_run)
+    monkeypatch.setattr(ref_runner, "reference_case_from_workload",
+                        lambda w, g: {"geometry": g, "spectrum": np.zeros(120)})
+    w = physics.workload("poly_grid_256")
+    args = types.SimpleNamespace(steps=4, warmup=2)
+    line = ref_runner.bench_line(args, w)
+    assert calls == [1, 1, 8, 24, 8, 24]
+    split = line["reference_split"]
+    assert abs(split["fixed_s"] - 5.0) < 1e-9 and abs(split["per_view_s"] - 0.25) < 1e-9
+    assert abs(line["value"] - 360 * 512 * 384 / (5.0 + 0.25 * 360)) < 1e-3
+    assert abs(line["ms_per_step"] - 1e3 * (5.0 + 0.25 * 16)) < 1e-6  # mean of the 8- and 24-view runs
+    assert line["config"]["views"] == 360 and line["steps"] == 4 and line["warmup"] == 2
+    assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "reference"
