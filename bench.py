@@ -10,8 +10,9 @@ per-pixel per-energy transmission.  A step is one full forward projection
 
   value  rays/s with inputs resident in HBM (CUDA events, L2 flushed between steps)
   e2e    rays/s through ctfp_forward_host: host volumes in, host I/IAbsorb out
-  roofline  the march kernel against the measured HBM copy bandwidth, with
-            32 B (8 FP32 corners) per voxel-sample of algorithmic traffic
+  roofline  the march kernel against its binding ceiling, the texture path's
+            measured peak, with 32 B (8 FP32 corners) per voxel-sample of
+            algorithmic traffic; the compulsory HBM bytes beside it
   cpu_baseline  the FP64 oracle on the host cores over a seeded ray subset
 
 Multi-GPU (torchrun): by default every rank projects its own seeded object
@@ -42,7 +43,7 @@ HBM_FALLBACK_GBS = 6650.0
 # (dram__bytes_read.sum + dram__bytes_write.sum) of k_forward on the 36-view
 # case of the same problem (poly_grid_256_v36, default launch shape): 5.95 GB +
 # 0.09 GB, scaled by 10 for 360 views (traffic grows with the views marched).
-TRAFFIC_PER_LAUNCH = {("poly_grid_256", "trilinear"): 60.37e9}
+TRAFFIC_PER_LAUNCH = {("poly_grid_256", "trilinear", "layered"): 60.37e9}
 BYTES_PER_VOXEL_SAMPLE = 32  # 8 FP32 corners, the reuse-free trilinear footprint
 
 
@@ -289,10 +290,14 @@ def main():
     ap.add_argument("--shard", default="objects", choices=["objects", "views"],
                     help="N > 1: each rank projects its own object (weak scaling) or a slab of one "
                          "object's views (strong scaling; the adjoint sums gradients with all-reduce)")
-    ap.add_argument("--sampler", default="layered", choices=["layered", "global", "brick", "axis"],
+    ap.add_argument("--sampler", default="axis", choices=["axis", "layered", "global", "brick"],
                     help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
                     help="problems in the uneven batch leg (0 skips it)")
+    ap.add_argument("--launch-shape", default=None,
+                    help="tile_u,tile_v,views_per_cta,min_ctas_per_sm for the march (instead of the autotuner)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other benchmark configurations (the `configs` block)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -346,8 +351,12 @@ def main():
     out = {"I": torch.empty((n_local, V, U), device=dev), "IAbsorb": torch.empty((n_local, V, U), device=dev)}
     stream = torch.cuda.current_stream()
     shape = {"tile_u": 16, "tile_v": 8, "views_per_cta": 2, "min_ctas_per_sm": 4, "source": "default"}
-    if not args.no_autotune:
-        r = pr.autotune(vols, n_sample_views=16)
+    if args.launch_shape:
+        tu, tv, vpc, mc = (int(x) for x in args.launch_shape.split(","))
+        pr.set_launch_shape(tu, tv, vpc, mc)
+        shape = {"tile_u": tu, "tile_v": tv, "views_per_cta": vpc, "min_ctas_per_sm": mc, "source": "--launch-shape"}
+    elif not args.no_autotune:
+        r = pr.autotune(vols, n_sample_views=64)
         shape = {k: r[k] for k in ("tile_u", "tile_v", "views_per_cta", "min_ctas_per_sm")}
         shape["source"] = "cache" if r["from_cache"] else "autotuned"
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
@@ -376,7 +385,7 @@ def main():
 
     # ---------------- optional empty-space skipping (not the headline) -------
     skip = None
-    if args.interp == "texture" or args.sampler == "layered":
+    if args.interp == "texture" or args.sampler in ("layered", "axis"):
         ref_I = out["I"].clone()
         pr.set_skip_empty(True)
         o2 = {"I": torch.empty_like(out["I"]), "IAbsorb": torch.empty_like(out["IAbsorb"])}
@@ -401,30 +410,41 @@ def main():
                         "occupancy rebuilt inside every timed step"}
         del o2, ref_I
 
-    # roofline: algorithmic bytes of the dominant kernel per launch
+    # roofline of the dominant kernel (the march): its algorithmic bytes are
+    # the 8 FP32 corners of every voxel-sample (32 B, reuse-free), which the
+    # texture path returns to registers; the binding ceiling is that path's
+    # rate for the march's own gathers, measured in this run (texture_roof).
+    # DRAM sees far fewer bytes (the texture cache serves neighbouring rays'
+    # shared corners): the compulsory HBM bytes (volumes once, outputs once)
+    # are reported beside it against the measured copy bandwidth.
     support = pr.count_support_samples()
     vs_launch = support * M * n_local // P  # sharded: this rank's share of the views, pro rata
     nominal_vs = M * rays * int(pr.info["intNum"])
-    peak, peak_kind = measured_peak_hbm()
-    achieved = vs_launch * BYTES_PER_VOXEL_SAMPLE / (ms / 1e3) / 1e9
+    hbm_peak, peak_kind = measured_peak_hbm()
     vs_rate = vs_launch / (ms / 1e3)
-    from ct_forward_projection_b200.projector import sampler_peak
-    tex_peak = None
-    if args.interp == "texture" or args.sampler == "layered":
-        tex_peak = sampler_peak(local, "tex3d" if args.interp == "texture" else "layered")
-    traffic = TRAFFIC_PER_LAUNCH.get((w.name, args.interp))
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind,
+    achieved = vs_rate * BYTES_PER_VOXEL_SAMPLE / 1e9
+    tex_peak, tex_src = texture_roof(pr, args.interp, args.sampler, local, {})
+    traffic = TRAFFIC_PER_LAUNCH.get((w.name, args.interp, args.sampler if args.interp != "texture" else "tex3d"))
+    nvox = int(np.prod(pr.shape_vol))
+    compulsory = M * nvox * 4 + n_local * U * V * 8
+    roofline = {"bound": "texture" if tex_peak else "hbm",
+                "achieved": achieved, "unit": "GB/s",
+                "peak": (tex_peak * BYTES_PER_VOXEL_SAMPLE / 1e9) if tex_peak else hbm_peak,
+                "frac": (vs_rate / tex_peak) if tex_peak else achieved / hbm_peak,
+                "peak_source": (tex_src + " x 32 B") if tex_peak else f"{peak_kind} HBM copy bandwidth",
+                "traffic": traffic,
+                "traffic_source": None if traffic is None else
+                    "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
+                    "the 36-view case of this workload, x10 for 360 views (the committed ncu summary of this kernel)",
                 "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_rate,
                 "nominal_voxel_samples_per_launch": nominal_vs,
-                "texture": None if tex_peak is None else {
-                    "peak_voxel_samples_per_s": tex_peak, "achieved_voxel_samples_per_s": vs_rate,
-                    "frac": vs_rate / tex_peak, "binding": True,
-                    "peak_source": "ctfp_sampler_peak, measured in this run"},
-                "roof_min_hbm32_tex": None if tex_peak is None else min(peak * 1e9 / BYTES_PER_VOXEL_SAMPLE, tex_peak),
-                "note": ("achieved = 32 B (reuse-free 8-corner footprint) x support voxel-samples / kernel time; "
-                         "the texture cache serves most corners, so DRAM traffic (ncu) is far below that and the "
-                         "binding ceiling is the texture path (texture.frac)")}
+                "hbm": {"compulsory_bytes_per_launch": compulsory,
+                        "achieved_GBs": compulsory / (ms / 1e3) / 1e9, "peak_GBs": hbm_peak,
+                        "frac": compulsory / (ms / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
+                        "note": "volumes read once + I and IAbsorb written once, against the HBM copy peak"},
+                "note": "achieved = 32 B (the 8 FP32 corners a trilinear sample reads, reuse-free) x support "
+                        "voxel-samples / kernel time; peak = the texture path's measured rate for the same "
+                        "gathers x 32 B"}
 
     # ---------------- end to end through ctfp_forward_host (e2e) ------------
     e2e = None
@@ -494,6 +514,11 @@ def main():
     if args.batch_items > 0:
         batch = batch_leg(args, ws, rank, local, stream)
 
+    # ---------------- the other configurations (rank 0, N = 1) -------------
+    configs = None
+    if rank == 0 and ws == 1 and not args.no_configs and not sharded:
+        configs = config_legs(args, local, stream, flush)
+
     # ---------------- CPU baseline (rank 0, N = 1) --------------------------
     cpu = None
     err = acc = None
@@ -528,6 +553,7 @@ def main():
             "fwd_adjoint": fa,
             "fwd_skip_empty": skip,
             "batch": batch,
+            "configs": configs,
             "launch_shape": shape,
             "gpu_launches": args.steps,
             "clocks": clk,
@@ -538,6 +564,145 @@ def main():
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+# The other benchmark configurations, each timed like the headline (CUDA
+# events on the launching stream, L2 flushed between steps) and checked
+# against the FP64 oracle on seeded rays: (workload, interp, timed steps,
+# forward + adjoint too).  poly_grid_256 in the two modes that reproduce the
+# reference's texture sampler; the single-material 128^3 case; the
+# differentiable three-material case; the large four-material case.
+CONFIG_LEGS = [("sinmat_nogrid_128", "trilinear", 5, False),
+               ("poly_grid_256", "texemu", 3, False),
+               ("poly_grid_256", "texture", 3, False),
+               ("diff_3mat_256", "trilinear", 3, True),
+               ("large_4mat_512", "trilinear", 2, True)]
+
+
+def texture_roof(pr, interp, sampler, local, cache):
+    """The march's binding ceiling in voxel-samples/s, measured in this run,
+    and how it was measured.  Layered sampler: ctfp_sampler_peak (two 4-texel
+    gathers per voxel-sample from an L1-resident texture, full warps, full
+    occupancy).  Axis sampler: the same lane-gather rate divided by the
+    gathers its march issues per voxel-sample on this geometry, counted by
+    active lane quads (ctfp_axis_gather_count; 0.5 = the layered sampler's
+    two full-warp gathers).  Hardware texture: one filtered tex3D fetch per
+    voxel-sample (ctfp_sampler_peak tex3d).  cache holds the probe results."""
+    from ct_forward_projection_b200.projector import sampler_peak
+    kind = "tex3d" if interp == "texture" else ("layered" if sampler in ("layered", "axis") else None)
+    if kind is None:
+        return None, None
+    if kind not in cache:
+        cache[kind] = sampler_peak(local, kind)
+    peak = cache[kind]
+    if interp != "texture" and sampler == "axis":
+        g = pr.axis_gather_count()
+        return peak * 0.5 / g, (f"measured in this run: ctfp_sampler_peak (layered, {peak:.3e}/s at 0.5 quad-gathers "
+                                f"per voxel-sample) x 0.5 / {g:.4f} quad-gathers per voxel-sample of this march "
+                                f"(ctfp_axis_gather_count)")
+    return peak, f"measured in this run: ctfp_sampler_peak ({kind})"
+
+
+def _accuracy(w, pr, vols, out, interp, n_rays=100000):
+    """Per-ray relative error of I and IAbsorb against the FP64 oracle on
+    seeded rays of the oracle's detector rows (max, p99): trilinear against the
+    exact oracle; the texture-unit modes against its texture emulation."""
+    from oracle import oracle as O
+    g = w.geometry
+    rows = oracle_rows(w)
+    W, tables = oracle_weights(w, rows)
+    rng = np.random.RandomState(17)
+    ids = _ray_ids(rng, g, rows, n_rays)
+    mode = O.TRILINEAR if interp == "trilinear" else O.TEXEMU
+    ref = O.forward(g, [v.cpu().numpy() for v in vols], w.mu_table(), W, mode, ids)
+    import torch
+    idx = torch.from_numpy(ids).to(out["I"].device)
+    acc = {}
+    for k, r in (("I", ref["I"]), ("IAbsorb", ref["IAbsorb"])):
+        got = out[k].reshape(-1)[idx].double().cpu().numpy()
+        acc[k] = _err_stats(np.abs(got - r) / np.maximum(np.abs(r), 1e-30))
+    acc["rays"] = int(len(ids))
+    acc["against"] = "FP64 oracle, " + ("exact trilinear" if mode == O.TRILINEAR else "texture-unit emulation")
+    acc["tables"] = tables
+    return acc
+
+
+def config_legs(args, local, stream, flush):
+    import torch
+
+    from ct_forward_projection_b200 import physics
+    from ct_forward_projection_b200.projector import Projector
+    dev = f"cuda:{local}"
+    res = {}
+    peaks = {}
+    for name, interp, steps, adjoint in CONFIG_LEGS:
+        key = f"{name}/{interp}"
+        try:
+            w = physics.workload(name)
+            vols = physics.phantom(w, dev)
+            M = len(vols)
+            pr = Projector(w.geometry, M, interp, local)
+            if interp != "texture":
+                pr.set_sampler(args.sampler)
+            pr.set_tables_from_workload(w)
+            P, V, U = pr.shape_proj
+            rays = P * U * V
+            out = {"I": torch.empty((P, V, U), device=dev), "IAbsorb": torch.empty((P, V, U), device=dev)}
+            pr.forward(vols, out=out)
+            ev = []
+            for s_ in range(steps):
+                flush.fill_(float(s_))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pr.forward(vols, out=out)
+                e1.record(stream)
+                ev.append((e0, e1))
+            torch.cuda.synchronize()
+            ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+            vs = pr.count_support_samples() * M
+            r = {"ms_per_forward": ms, "rays_per_s": rays / (ms / 1e3), "voxel_samples_per_s": vs / (ms / 1e3),
+                 "rays": rays, "voxel_samples": vs, "steps": steps,
+                 "volume": list(pr.shape_vol[::-1]), "materials": M, "views": P, "detector": [U, V], "energies": pr.E,
+                 "sampler": "tex3d" if interp == "texture" else args.sampler}
+            tpeak, tsrc = texture_roof(pr, interp, args.sampler, local, peaks)
+            if tpeak:
+                r["texture_frac"] = r["voxel_samples_per_s"] / tpeak
+                r["texture_peak_voxel_samples_per_s"] = tpeak
+                r["texture_peak_source"] = tsrc
+            if adjoint:
+                L = torch.empty((P, V, U, M), device=dev)
+                T = pr.forward([v * 0.97 for v in vols])["I"]
+                logT = torch.log(T)
+                del T
+                grads = [torch.zeros_like(v) for v in vols]
+
+                def fa_step():
+                    pr.forward(vols, out={**out, "L": L})
+                    rr = torch.log(out["I"]) - logT
+                    pr.backward(L, 2.0 * rr / out["I"], None, grads)
+
+                fa_step()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(steps):
+                    fa_step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                fa_ms = e0.elapsed_time(e1) / steps
+                r["fwd_adjoint"] = {"ms_per_step": fa_ms, "rays_per_s": rays / (fa_ms / 1e3),
+                                    "step": "forward with checkpoint, dLoss/dI of sum (log I - log T)^2 in torch, "
+                                            "adjoint and fold; T = projection of the phantom x 0.97"}
+                del L, logT, grads
+            if not args.no_cpu:
+                r["accuracy_vs_fp64_oracle"] = _accuracy(w, pr, vols, out, interp)
+            pr.close()
+            del vols, out
+            torch.cuda.empty_cache()
+            res[key] = r
+        except Exception as e:  # a failed leg is reported, the bench line still prints
+            res[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+    return res
 
 
 def fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays, fa_ms, ws, stream):
@@ -687,7 +852,8 @@ def batch_leg(args, ws, rank, local, stream):
     return {
         "items": len(wl), "rays_per_pass": rays, "work_units": info["units"],
         "persistent_grid": [info["grid_forward"], info["grid_adjoint"]],
-        "unit_tile": [unit_shape["tile_u"], unit_shape["tile_v"]],
+        "unit_tile": {"fwd": [unit_shape["fwd_tile_u"], unit_shape["fwd_tile_v"]],
+                      "fwd_adjoint": [unit_shape["tile_u"], unit_shape["tile_v"]]},
         "fwd": {"loop_rays_s": n_rays / (t_loop_f / 1e3), "batched_rays_s": n_rays / (t_b_f / 1e3),
                 "loop_ms": t_loop_f, "batched_ms": t_b_f, "speedup": t_loop_f / t_b_f},
         "fwd_adjoint": {"loop_rays_s": n_rays / (t_loop_fa / 1e3), "batched_rays_s": n_rays / (t_b_fa / 1e3),

@@ -84,6 +84,7 @@ _SIGNATURES = {
     "ctfp_line_integrals_adjoint": (C.c_int, [_P, _P, _P, _P]),
     "ctfp_sample_volume": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int32, _P, C.c_int64, _P, _P]),
     "ctfp_count_support_samples": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "ctfp_axis_gather_count": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "ctfp_forward_host": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "ctfp_build_grid_table": (C.c_int, [C.POINTER(Geometry), C.POINTER(GridParams), C.c_int32, _P, _P, C.c_int32,
                                         _P, _P]),
@@ -101,6 +102,8 @@ _SIGNATURES = {
     "ctfp_batch_info": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ctfp_batch_set_shape": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "ctfp_batch_autotune": (C.c_int, [_P, _P, _P, _P, _P]),
+    "ctfp_batch_get_shapes": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32)]),
     "ctfp_last_error_string": (C.c_char_p, []),
     "ctfp_version": (C.c_char_p, []),
 }

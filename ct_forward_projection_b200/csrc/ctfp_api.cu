@@ -249,20 +249,24 @@ ctfp_status make_layered_rw(size_t width, size_t height, size_t layers, cudaArra
 }
 
 // The axis sampler's two copies per material: layered along x (texels
-// (y, z), a layer per x) and along y (texels (x, z), a layer per y).
+// (y, z), texture layer x + 1) and along y (texels (x, z), layer y + 1), each
+// with a zero layer before and after the volume.
 ctfp_status make_axis(ctfp_plan* p)
 {
     const size_t nx = (size_t)p->geom.pNumX, ny = (size_t)p->geom.pNumY, nz = (size_t)p->geom.pNumZ;
     for (int m = 0; m < p->M; m++) {
         if (p->xarr[m]) continue;
-        ctfp_status st = make_layered_rw(ny, nz, nx, p->xarr[m], p->xtex[m], p->xsurf[m]);
-        if (st == CTFP_OK) st = make_layered_rw(nx, nz, ny, p->yarr[m], p->ytex[m], p->ysurf[m]);
+        ctfp_status st = make_layered_rw(ny, nz, nx + 2, p->xarr[m], p->xtex[m], p->xsurf[m]);
+        if (st == CTFP_OK) st = make_layered_rw(nx, nz, ny + 2, p->yarr[m], p->ytex[m], p->ysurf[m]);
         if (st != CTFP_OK) return st;
+        CTFP_CUDA(launch_axis_zero_pads((int)nx, (int)ny, (int)nz, p->xsurf[m], p->ysurf[m], 0));
+        CTFP_CUDA(cudaStreamSynchronize(0));
     }
     return CTFP_OK;
 }
 
-bool axis_fits(const ctfp_geometry& g) { return g.pNumX <= 2048 && g.pNumY <= 2048 && g.pNumZ <= 32768; }
+// two pad layers each: at most 2046 voxel layers along x and y
+bool axis_fits(const ctfp_geometry& g) { return g.pNumX <= 2046 && g.pNumY <= 2046 && g.pNumZ <= 32768; }
 
 void free_textures(ctfp_plan* p)
 {
@@ -511,10 +515,12 @@ ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_
     }
     gp.trig = p->d_trig;
     gp.trigf = p->d_trigf;
-    // layered 2D textures hold at most 2048 layers
-    if (g->pNumZ > 2048) p->sampler = SAMPLER_GLOBAL;
-    if (uses_layered(p)) {
-        st = make_layered(p);
+    // default corner source: the axis sampler (fastest measured); layered
+    // textures hold at most 2048 layers, so past its limits the z-layered
+    // sampler, past those the caller's volumes
+    p->sampler = axis_fits(*g) ? SAMPLER_AXIS : (g->pNumZ <= 2048 ? SAMPLER_LAYERED : SAMPLER_GLOBAL);
+    if (uses_layered(p) || uses_axis(p)) {
+        st = uses_axis(p) ? make_axis(p) : make_layered(p);
         if (st != CTFP_OK) {
             std::string msg = g_last_error;
             ctfp_plan_destroy(p);
@@ -594,7 +600,7 @@ ctfp_status ctfp_plan_set_sampler(ctfp_plan* p, int32_t sampler)
     if (sampler == CTFP_SAMPLER_LAYERED && p->geom.pNumZ > 2048)
         return fail(CTFP_UNSUPPORTED, "layered sampler holds at most 2048 z slices");
     if (sampler == CTFP_SAMPLER_AXIS && !axis_fits(p->geom))
-        return fail(CTFP_UNSUPPORTED, "axis sampler needs pNumX, pNumY <= 2048 and pNumZ <= 32768");
+        return fail(CTFP_UNSUPPORTED, "axis sampler needs pNumX, pNumY <= 2046 and pNumZ <= 32768");
     DeviceScope ds(p->device);
     p->sampler = sampler;
     if (uses_layered(p)) return make_layered(p);
@@ -932,6 +938,24 @@ ctfp_status ctfp_sample_volume(const float* volume, int64_t nx, int64_t ny, int6
     return CTFP_OK;
 }
 
+ctfp_status ctfp_axis_gather_count(ctfp_plan* p, double* quad_gathers_per_sample)
+{
+    if (!p || !quad_gathers_per_sample) return fail(CTFP_INVALID_ARG, "NULL argument");
+    if (p->interp == INTERP_TEXTURE) return fail(CTFP_UNSUPPORTED, "the hardware texture mode has no gathers");
+    DeviceScope ds(p->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "cudaSetDevice");
+    unsigned long long* d = nullptr;
+    CTFP_CUDA(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = launch_axis_gather_count(p->gp, p->interp, p->shape, d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "ctfp_axis_gather_count");
+    *quad_gathers_per_sample = h[1] ? (double)h[0] / (double)h[1] : 0.0;
+    return CTFP_OK;
+}
+
 ctfp_status ctfp_count_support_samples(ctfp_plan* p, int64_t* out)
 {
     if (!p || !out) return fail(CTFP_INVALID_ARG, "NULL argument");
@@ -959,6 +983,8 @@ const float* plan_mu(const ctfp_plan* p) { return p->d_mu; }
 const float* plan_W(const ctfp_plan* p) { return p->d_W; }
 LaunchShape& plan_shape(ctfp_plan* p) { return p->shape; }
 cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m) { return p->ltex[m]; }
+cudaTextureObject_t plan_xtex(const ctfp_plan* p, int m) { return p->xtex[m]; }
+cudaTextureObject_t plan_ytex(const ctfp_plan* p, int m) { return p->ytex[m]; }
 cudaTextureObject_t plan_tex(const ctfp_plan* p, int m) { return p->tex[m]; }
 MarchParams plan_march_params(const ctfp_plan* p) { return base_params(p); }
 const ctfp_geometry& plan_geometry(const ctfp_plan* p) { return p->geom; }
@@ -1045,7 +1071,8 @@ extern "C" ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* p, int32_t tile_u, 
     if (!p) return fail(CTFP_INVALID_ARG, "plan is NULL");
     if (tile_u < 1 || tile_v < 1 || tile_u * tile_v > 256 || (tile_u * tile_v) % 32 != 0 || views_per_cta < 1)
         return fail(CTFP_INVALID_ARG, "tile_u*tile_v must be a multiple of 32 and at most 256");
-    if (min_ctas_per_sm < 2 || min_ctas_per_sm > 4) return fail(CTFP_INVALID_ARG, "min_ctas_per_sm must be 2, 3 or 4");
+    if (min_ctas_per_sm < 2 || min_ctas_per_sm > 5)
+        return fail(CTFP_INVALID_ARG, "min_ctas_per_sm must be 2, 3, 4 or 5 (5: the axis sampler only; others use 4)");
     if (tile_u * tile_v * min_ctas_per_sm > 2048)
         return fail(CTFP_INVALID_ARG, "tile_u*tile_v*min_ctas_per_sm exceeds 2048 threads per SM");
     p->shape.tile_u = tile_u;

@@ -103,7 +103,7 @@ void append_file_cache(const std::string& key, const Entry& e)
 bool valid_shape(const LaunchShape& s)
 {
     const int t = s.tile_u * s.tile_v;
-    return t >= 32 && t <= 256 && t % 32 == 0 && s.views_per_cta >= 1 && s.min_ctas >= 2 && s.min_ctas <= 4 &&
+    return t >= 32 && t <= 256 && t % 32 == 0 && s.views_per_cta >= 1 && s.min_ctas >= 2 && s.min_ctas <= 5 &&
            t * s.min_ctas <= 2048;
 }
 

@@ -1,0 +1,241 @@
+// ctfp_axis.cuh — the axis sampler's ray march (SAMPLER_AXIS), shared by the
+// plan kernels (k_forward_axis) and the batched persistent kernels.
+#pragma once
+
+#include "ctfp_device.cuh"
+
+namespace ctfp {
+
+// Brick occupancy for empty-space skipping as a march reads it: bricks of
+// 2^shift voxels per axis, occ_x x occ_y per z layer of bricks.
+struct OccView {
+    const uint8_t* occ;
+    int occ_x, occ_y, nx, ny, nz, shift;
+    // whether the footprint with base corner c can read a non-zero voxel;
+    // bases outside [-1, n - 1] read only the border
+    __device__ __forceinline__ bool occupied(const Corner& c) const
+    {
+        const unsigned x = (unsigned)(c.ix + 1), y = (unsigned)(c.iy + 1), z = (unsigned)(c.iz + 1);
+        if (x > (unsigned)nx || y > (unsigned)ny || z > (unsigned)nz) return false;
+        const size_t b = ((size_t)(z >> shift) * occ_y + (y >> shift)) * occ_x + (x >> shift);
+        return __ldg(occ + b) != 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Axis sampler (SAMPLER_AXIS).  A view whose central ray runs mostly along x
+// reads the copies layered along x (layer = x index, texel (y, z)); any other
+// view reads the copies layered along y (layer = y, texel (x, z)).  A sample's
+// footprint is then two 2x2 gathers, layers L and L + 1, at the in-layer base
+// (a, b).  Consecutive samples lie half a voxel apart, mostly along the layer
+// axis, so a sample usually has the previous sample's footprint or the same
+// in-layer base one layer on.  Each ray keeps two gathers per material in
+// registers, slot 0 for the even and slot 1 for the odd layer of its current
+// pair, and a sample fetches only a slot whose layer or base changed: nothing,
+// one layer (the other slot keeps its layer), or both when the in-layer base
+// moved.  Which slot is the lower layer depends on L's parity, which selects
+// the layer-axis weights rather than moving values between registers.  The
+// texture unit spends its time per active quad of 4 lanes, so the lane layout
+// (k_forward_axis) puts each quad on 4 adjacent detector rows of one column:
+// their rays cross layer and in-layer cell boundaries at nearly the same
+// samples and skip their gathers together.  The copies carry one zero layer
+// before and after the volume (texture layer = layer + 1), and the unit clamps
+// layer indices, so a footprint overhanging the volume reads zeros there with
+// no test.
+
+// In-layer bilinear value of one gather q (tld4 order: x = (a, b+1),
+// y = (a+1, b+1), z = (a+1, b), w = (a, b)) with weights (ua, wa) on the
+// in-layer axis a and (ub, wb) on z.
+__device__ __forceinline__ float bilinear_quad(const float4& q, float ua, float wa, float ub, float wb)
+{
+    const float r0 = fmaf(q.z, wa, q.w * ua);
+    const float r1 = fmaf(q.y, wa, q.x * ua);
+    return fmaf(r1, wb, r0 * ub);
+}
+
+// The gathers one ray holds: the layers in slot 0 (even) and slot 1 (odd)
+// and their in-layer base; the sentinel layer matches no footprint (bases are
+// >= -2).  fetch() takes the next footprint (lower layer lc, in-layer base
+// (a, b)), says which slots must be fetched (their texture layers are e0 + 1
+// and e1 + 1: layer 0 of a copy is its zero pad) and holds the new pair.
+struct AxisHold {
+    int h0 = -1000000000, h1 = -1000000000, ca = 0, cb = 0;
+    __device__ __forceinline__ void fetch(int lc, int a, int b, int& e0, int& e1, bool& n0, bool& n1)
+    {
+        const int par = lc & 1;
+        e0 = lc + par;       // the even layer of {lc, lc + 1}
+        e1 = lc + 1 - par;   // the odd one
+        const bool base = (a == ca) & (b == cb);
+        n0 = !(base & (h0 == e0));
+        n1 = !(base & (h1 == e1));
+        h0 = e0;
+        h1 = e1;
+        ca = a;
+        cb = b;
+    }
+};
+
+// The footprint of sample i in the axis sampler's terms: lower layer, in-layer
+// base and the corner (TRILINEAR: from the stepped FP64 coordinates).
+template <int MODE>
+__device__ __forceinline__ Corner axis_corner(const GeomParams& g, const RayRef32& r, int i, double& cx, double& cy,
+                                              double& cz, const RaySeg& s)
+{
+    if (MODE == INTERP_TRILINEAR) {
+        const Corner c = corner_of<INTERP_TRILINEAR>(cx, cy, cz);
+        cx += s.bx;
+        cy += s.by;
+        cz += s.bz;
+        return c;
+    }
+    return corner_tex(ref32_coords(g, r, i));
+}
+
+// L_m for one ray with the axis sampler (AX 0: layered along x, 1: along y).
+// Each ray is marched on its own (from its own first sample), so its result
+// does not depend on the launch shape.  (Stepping a warp's lanes through
+// common sample indices instead, from the earliest entry to the latest exit
+// among them, measured 3 % slower on poly_grid_256: the extra iterations
+// cost more than the gathers the tighter lockstep saves.)
+template <int M, int MODE, int AX, bool SKIP>
+__device__ __forceinline__ void march_ray_axis(const GeomParams& g, const cudaTextureObject_t* xtex,
+                                               const cudaTextureObject_t* ytex, const OccView& occ, int p, int v,
+                                               int u, float* L)
+{
+    const RaySeg s = ray_segment(g, p, v, u);
+    RayRef32 r;
+    if (MODE != INTERP_TRILINEAR) r = ray_ref32(g, p, v, u);
+    const cudaTextureObject_t* tx = AX == 0 ? xtex : ytex;
+    float acc[M], cmp[M];
+    float4 q0[M], q1[M];  // slot 0: the even layer of the pair, slot 1: the odd one
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        acc[m] = 0.f;
+        cmp[m] = 0.f;
+        q0[m] = q1[m] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    AxisHold hold;
+    // FP64 coordinates stepped by one sample (c += b: within 1e-10 voxel of
+    // a + b i over any ray); samples summed in blocks of kBlock in FP32, the
+    // block sums compensated (Kahan)
+    double cx = fma((double)s.i0, s.bx, s.ax), cy = fma((double)s.i0, s.by, s.ay), cz = fma((double)s.i0, s.bz, s.az);
+    constexpr int kBlock = 16;
+    for (int ib = s.i0; ib < s.i1; ib += kBlock) {
+    const int ie = min(ib + kBlock, s.i1);
+    float blk[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) blk[m] = 0.f;
+#pragma unroll 2
+    for (int i = ib; i < ie; i++) {
+        const Corner c = axis_corner<MODE>(g, r, i, cx, cy, cz, s);
+        if (SKIP && !occ.occupied(c)) continue;
+        const int lc = AX == 0 ? c.ix : c.iy;
+        const int a = AX == 0 ? c.iy : c.ix;
+        const int b = c.iz;
+        const int par = lc & 1;
+        int e0, e1;
+        bool n0, n1;
+        hold.fetch(lc, a, b, e0, e1, n0, n1);
+        const float fa = (float)(a + 1), fb = (float)(b + 1);
+        if (n0) {
+#pragma unroll
+            for (int m = 0; m < M; m++) q0[m] = gather_layer_cond(tx[m], e0 + 1, fa, fb);
+        }
+        if (n1) {
+#pragma unroll
+            for (int m = 0; m < M; m++) q1[m] = gather_layer_cond(tx[m], e1 + 1, fa, fb);
+        }
+        if (MODE == INTERP_TRILINEAR) {
+            // weights of the lower and upper layer, assigned to the slots by parity
+            const float wl = AX == 0 ? c.ux : c.uy, wh = AX == 0 ? c.wx : c.wy;
+            const float w0 = par ? wh : wl, w1 = par ? wl : wh;
+            const float ua = AX == 0 ? c.uy : c.ux, wa = AX == 0 ? c.wy : c.wx;
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const float s0 = bilinear_quad(q0[m], ua, wa, c.uz, c.wz);
+                const float s1 = bilinear_quad(q1[m], ua, wa, c.uz, c.wz);
+                blk[m] += fmaf(s1, w1, s0 * w0);
+            }
+        } else {
+            // the texture unit's 8 weights (k = dz*4 + dy*2 + dx); the layer
+            // axis is bit 0 of k (x) or bit 1 (y); slot 0 is the lower layer
+            // when par = 0
+            float w[8];
+            texunit_weights(c.qx, c.qy, c.qz, w);
+            constexpr int lb = AX == 0 ? 1 : 2;  // the layer bit of k
+            constexpr int ab = AX == 0 ? 2 : 1;  // the in-layer axis bit of k
+            float g0[4], g1[4];  // weights of slot 0 / slot 1 texels (a, b), (a+1, b), (a, b+1), (a+1, b+1)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int k = (j & 2 ? 4 : 0) + (j & 1 ? ab : 0);
+                g0[j] = par ? w[k + lb] : w[k];
+                g1[j] = par ? w[k] : w[k + lb];
+            }
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                float v = g0[0] * q0[m].w;
+                v = fmaf(g0[1], q0[m].z, v);
+                v = fmaf(g0[2], q0[m].x, v);
+                v = fmaf(g0[3], q0[m].y, v);
+                v = fmaf(g1[0], q1[m].w, v);
+                v = fmaf(g1[1], q1[m].z, v);
+                v = fmaf(g1[2], q1[m].x, v);
+                v = fmaf(g1[3], q1[m].y, v);
+                blk[m] += v;
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], blk[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) L[m] = g.dx * (acc[m] - cmp[m]);
+}
+
+// The gathers the axis march of one ray issues, as the texture unit sees
+// them: the warp's lanes run the march loop in step, lane k at iteration j on
+// its own sample i0_k + j, and per iteration and slot the lane quads with a
+// lane that fetches are counted (out[0], per material), with the lanes'
+// samples (out[1], per material).  The first lane of warp_mask returns the
+// warp's totals.  Same footprints and hold logic as march_ray_axis.
+template <int MODE, int AX>
+__device__ __forceinline__ void count_ray_axis(const GeomParams& g, int p, int v, int u, unsigned warp_mask,
+                                               unsigned long long* out)
+{
+    const RaySeg s = ray_segment(g, p, v, u);
+    RayRef32 r;
+    if (MODE != INTERP_TRILINEAR) r = ray_ref32(g, p, v, u);
+    const int len = s.i1 - s.i0;
+    const int wlen = __reduce_max_sync(warp_mask, len > 0 ? len : 0);
+    double cx = fma((double)s.i0, s.bx, s.ax), cy = fma((double)s.i0, s.by, s.ay), cz = fma((double)s.i0, s.bz, s.az);
+    AxisHold hold;
+    unsigned long long quads = 0, samples = 0;
+    for (int j = 0; j < wlen; j++) {
+        bool n0 = false, n1 = false;
+        if (j < len) {
+            const Corner c = axis_corner<MODE>(g, r, s.i0 + j, cx, cy, cz, s);
+            int e0, e1;
+            hold.fetch(AX == 0 ? c.ix : c.iy, AX == 0 ? c.iy : c.ix, c.iz, e0, e1, n0, n1);
+            samples++;
+        }
+        // quads with a fetching lane: OR the 4 lanes of each quad onto its first lane
+        unsigned b0 = __ballot_sync(warp_mask, n0), b1 = __ballot_sync(warp_mask, n1);
+        b0 = (b0 | (b0 >> 1) | (b0 >> 2) | (b0 >> 3)) & 0x11111111u;
+        b1 = (b1 | (b1 >> 1) | (b1 >> 2) | (b1 >> 3)) & 0x11111111u;
+        quads += (unsigned long long)(__popc(b0) + __popc(b1));
+    }
+    samples = __reduce_add_sync(warp_mask, (unsigned)samples);
+    out[0] = quads;
+    out[1] = samples;
+}
+
+// Whether view p reads the x-layered copies: its central ray (direction
+// (cos th, -sin th) in the volume's x-y plane) advances at least as many x
+// voxels as y voxels per step.
+__device__ __forceinline__ bool axis_is_x(const GeomParams& g, int p)
+{
+    const double2 cs = g.trig[p];
+    return fabs(cs.x) * (double)g.pSizeY >= fabs(cs.y) * (double)g.pSizeX;
+}
+
+}  // namespace ctfp

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/ctfp.h"
+#include "ctfp_axis.cuh"
 #include "ctfp_kernels.cuh"
 
 namespace ctfp {
@@ -38,6 +39,8 @@ int plan_energies(const ctfp_plan* p);
 const float* plan_mu(const ctfp_plan* p);
 const float* plan_W(const ctfp_plan* p);
 cudaTextureObject_t plan_ltex(const ctfp_plan* p, int m);
+cudaTextureObject_t plan_xtex(const ctfp_plan* p, int m);
+cudaTextureObject_t plan_ytex(const ctfp_plan* p, int m);
 cudaTextureObject_t plan_tex(const ctfp_plan* p, int m);
 ctfp_status plan_upload(ctfp_plan* p, const float* const* volumes, cudaStream_t st);
 }  // namespace ctfp
@@ -56,6 +59,8 @@ constexpr int kWarps = 2, kThreads = 32 * kWarps;
 struct ItemDesc {
     GeomParams g;
     cudaTextureObject_t ltex[kMaxM];   // layered textures (TRILINEAR, TEXEMU)
+    cudaTextureObject_t xtex[kMaxM];   // the axis sampler's x- and y-layered copies (TRILINEAR, TEXEMU)
+    cudaTextureObject_t ytex[kMaxM];
     cudaTextureObject_t tex[kMaxM];    // 3D textures (TEXTURE: the reference's own sampler)
     const float* mu;   // [E][M]
     const float* W;    // [E][V][U]
@@ -103,11 +108,20 @@ __device__ __forceinline__ Corner batch_corner(const ItemDesc& it, const RaySeg&
     return corner_tex(ref32_coords(it.g, r, i));
 }
 
-// Path integrals of one ray: the layered sampler, or in TEXTURE mode the
-// hardware tex3D at the reference's FP32 coordinates (as k_forward).
-template <int M, int MODE>
-__device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s, const RayRef32& r, float* L)
+// Path integrals of one ray: the axis sampler (AXIS), the layered sampler, or
+// in TEXTURE mode the hardware tex3D at the reference's FP32 coordinates (as
+// k_forward).
+template <int M, int MODE, bool AXIS>
+__device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s, const RayRef32& r, int p, int v,
+                                            int u, float* L)
 {
+    if (AXIS && MODE != INTERP_TEXTURE) {
+        const OccView none{nullptr, 0, 0, 0, 0, 0, 0};
+        constexpr int AM = MODE == INTERP_TEXTURE ? INTERP_TEXEMU : MODE;  // (not instantiated for TEXTURE)
+        if (axis_is_x(it.g, p)) march_ray_axis<M, AM, 0, false>(it.g, it.xtex, it.ytex, none, p, v, u, L);
+        else march_ray_axis<M, AM, 1, false>(it.g, it.xtex, it.ytex, none, p, v, u, L);
+        return;
+    }
     float acc[M], cmp[M];
 #pragma unroll
     for (int m = 0; m < M; m++) { acc[m] = 0.f; cmp[m] = 0.f; }
@@ -145,7 +159,7 @@ __device__ __forceinline__ void batch_scatter(const ItemDesc& it, const RaySeg& 
 
 // One ray.  ADJOINT: the fused forward + loss + adjoint; returns the ray's
 // loss term.
-template <int M, int MODE, bool ADJOINT>
+template <int M, int MODE, bool ADJOINT, bool AXIS>
 __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_mu, int p, int v, int u)
 {
     const int64_t npix = (int64_t)it.g.U * it.g.V;
@@ -155,7 +169,7 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     RayRef32 r;
     if (MODE != INTERP_TRILINEAR) r = ray_ref32(it.g, p, v, u);
     float L[M];
-    batch_march<M, MODE>(it, s, r, L);
+    batch_march<M, MODE, AXIS>(it, s, r, p, v, u, L);
     float sI = 0.f, cI = 0.f, sA = 0.f, cA = 0.f, S[M];
 #pragma unroll
     for (int m = 0; m < M; m++) S[m] = 0.f;
@@ -215,7 +229,7 @@ struct BatchBudget {
                                     : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 12 : 10));
 };
 
-template <int M, int MODE, bool ADJOINT>
+template <int M, int MODE, bool ADJOINT, bool AXIS>
 __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb) k_batch(const GroupArgs a)
 {
     __shared__ float s_mu[CTFP_MAX_ENERGIES * M];
@@ -256,10 +270,19 @@ __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb)
             tv = t / it.tiles_u;
             tu = t % it.tiles_u;
         }
-        const int u = (tu << a.tu_shift) + (threadIdx.x & ((1 << a.tu_shift) - 1));
-        const int v = tv * (kThreads >> a.tu_shift) + (threadIdx.x >> a.tu_shift);
+        int u, v;
+        const int tile_u = 1 << a.tu_shift, tile_v = kThreads >> a.tu_shift;
+        if (AXIS && tile_v % 4 == 0 && tile_u <= 16) {
+            // the axis sampler's lane quads run down 4 detector rows
+            const int q = threadIdx.x >> 2;
+            u = tu * tile_u + q % tile_u;
+            v = tv * tile_v + 4 * (q / tile_u) + (threadIdx.x & 3);
+        } else {
+            u = tu * tile_u + (threadIdx.x & (tile_u - 1));
+            v = tv * tile_v + (threadIdx.x >> a.tu_shift);
+        }
         float loss = 0.f;
-        if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT>(it, s_mu, p, v, u);
+        if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT, AXIS>(it, s_mu, p, v, u);
         if (ADJOINT && it.loss) {
             for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
             if (lane == 0) s_loss[warp] = loss;
@@ -300,21 +323,23 @@ __global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long
 using KernelFn = void (*)(GroupArgs);
 
 template <int M, bool ADJOINT>
-KernelFn kernel_for_m(int interp)
+KernelFn kernel_for_m(int interp, bool axis)
 {
-    if (interp == INTERP_TRILINEAR) return k_batch<M, INTERP_TRILINEAR, ADJOINT>;
-    if (interp == INTERP_TEXEMU) return k_batch<M, INTERP_TEXEMU, ADJOINT>;
-    return k_batch<M, INTERP_TEXTURE, ADJOINT>;
+    if (interp == INTERP_TRILINEAR)
+        return axis ? k_batch<M, INTERP_TRILINEAR, ADJOINT, true> : k_batch<M, INTERP_TRILINEAR, ADJOINT, false>;
+    if (interp == INTERP_TEXEMU)
+        return axis ? k_batch<M, INTERP_TEXEMU, ADJOINT, true> : k_batch<M, INTERP_TEXEMU, ADJOINT, false>;
+    return k_batch<M, INTERP_TEXTURE, ADJOINT, false>;
 }
 
 template <bool ADJOINT>
-KernelFn kernel_for(int M, int interp)
+KernelFn kernel_for(int M, int interp, bool axis)
 {
     switch (M) {
-        case 1: return kernel_for_m<1, ADJOINT>(interp);
-        case 2: return kernel_for_m<2, ADJOINT>(interp);
-        case 3: return kernel_for_m<3, ADJOINT>(interp);
-        default: return kernel_for_m<4, ADJOINT>(interp);
+        case 1: return kernel_for_m<1, ADJOINT>(interp, axis);
+        case 2: return kernel_for_m<2, ADJOINT>(interp, axis);
+        case 3: return kernel_for_m<3, ADJOINT>(interp, axis);
+        default: return kernel_for_m<4, ADJOINT>(interp, axis);
     }
 }
 
@@ -323,13 +348,17 @@ KernelFn kernel_for(int M, int interp)
 struct ctfp_batch {
     int n = 0;
     int device = 0;
-    int tile_u = kTU, tile_v = kTV;  // rays of a work unit (ctfp_batch_set_shape / ctfp_batch_autotune)
+    // rays of a work unit, per kind of call (0: forward, 1: forward + adjoint),
+    // set by ctfp_batch_set_shape (both) or tuned per kind by ctfp_batch_autotune
+    int tile_u[2] = {kTU, kTU}, tile_v[2] = {kTV, kTV};
+    int laid_out = -1;  // the kind the units are currently laid out for
     std::vector<ctfp_plan*> plans;
     std::vector<int> order;            // item slot -> plan index (grouped, cost order within a group)
+    std::vector<bool> item_axis;       // slot -> the plan marches the axis sampler's copies
     std::vector<long long> vox0;       // first voxel of each slot in the fold's flat index
     std::vector<ItemDesc> items;       // tables of the current call
     struct Group {
-        int M, interp, first, count;
+        int M, interp, axis, first, count;
         long long begin, end;
         int grid[2];                   // persistent grid: forward, forward + adjoint
     };
@@ -392,8 +421,9 @@ ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>&
         const ctfp_batch::Group& G = b->groups[gi];
         // tuning runs the first 1/tune_div of each group's queue: its largest items
         const long long end = tune_div > 0 ? G.begin + std::max(1LL, (G.end - G.begin) / tune_div) : G.end;
-        GroupArgs a{table, G.first, G.count, G.begin, end, b->d_counter + gi, __builtin_ctz((unsigned)b->tile_u)};
-        KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp) : kernel_for<false>(G.M, G.interp);
+        GroupArgs a{table, G.first, G.count, G.begin, end, b->d_counter + gi,
+                    __builtin_ctz((unsigned)b->tile_u[adjoint ? 1 : 0])};
+        KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp, G.axis) : kernel_for<false>(G.M, G.interp, G.axis);
         fn<<<G.grid[adjoint ? 1 : 0], kThreads, 0, st>>>(a);
         BATCH_CUDA(cudaGetLastError());
     }
@@ -461,13 +491,19 @@ struct DevScope {
 
 bool batchable(const ctfp_plan* p)
 {
-    return (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) == SAMPLER_LAYERED) && !plan_geom(p).fspot;
+    return (plan_interp(p) == INTERP_TEXTURE || plan_sampler(p) == SAMPLER_LAYERED ||
+            plan_sampler(p) == SAMPLER_AXIS) &&
+           !plan_geom(p).fspot;
 }
 
-// Unit counts and queue ranges for the batch's unit shape: item s holds
-// tiles_u x tiles_v x P units, numbered after the items before it.
-void layout_units(ctfp_batch* b)
+// Whether the item marches the axis sampler's copies.
+bool uses_axis(const ctfp_plan* p) { return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_AXIS; }
+
+// Unit counts and queue ranges for the unit shape of one kind of call: item s
+// holds tiles_u x tiles_v x P units, numbered after the items before it.
+void layout_units(ctfp_batch* b, int kind)
 {
+    b->laid_out = kind;
     long long unit = 0;
     size_t gi = 0;
     for (int s = 0; s < b->n; s++) {
@@ -476,26 +512,30 @@ void layout_units(ctfp_batch* b)
         while (gi + 1 < b->groups.size() && s >= b->groups[gi + 1].first) gi++;
         if (s == b->groups[gi].first) b->groups[gi].begin = unit;
         it.unit0 = unit;
-        it.units = (long long)((g.U + b->tile_u - 1) / b->tile_u) * ((g.V + b->tile_v - 1) / b->tile_v) * g.P;
+        it.units = (long long)((g.U + b->tile_u[kind] - 1) / b->tile_u[kind]) *
+                   ((g.V + b->tile_v[kind] - 1) / b->tile_v[kind]) * g.P;
         unit += it.units;
         b->groups[gi].end = unit;
     }
     b->total_units = unit;
 }
 
-// Fills the per-call tables from the plans' current state.
-ctfp_status fill_items(ctfp_batch* b)
+// Fills the per-call tables from the plans' current state, with the units
+// laid out for this kind of call.
+ctfp_status fill_items(ctfp_batch* b, int kind)
 {
+    if (b->laid_out != kind) layout_units(b, kind);
     for (int s = 0; s < b->n; s++) {
         ctfp_plan* p = b->plans[(size_t)b->order[(size_t)s]];
         if (!batchable(p))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need the layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
+                         "batched items need the axis or layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
         if (plan_energies(p) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
         ItemDesc& it = b->items[(size_t)s];
         const long long unit0 = it.unit0, units = it.units;
         const int M = it.M, interp = it.interp;
-        if (plan_materials(p) != M || plan_interp(p) != interp)
+        const bool axis = b->item_axis[(size_t)s];
+        if (plan_materials(p) != M || plan_interp(p) != interp || uses_axis(p) != axis)
             return bfail(CTFP_INVALID_ARG, "a plan's sampler mode changed after ctfp_batch_create");
         std::memset(&it, 0, sizeof(it));
         it.g = plan_geom(p);
@@ -506,11 +546,13 @@ ctfp_status fill_items(ctfp_batch* b)
         it.W = plan_W(p);
         for (int m = 0; m < it.M; m++) {
             it.ltex[m] = plan_ltex(p, m);
+            it.xtex[m] = plan_xtex(p, m);
+            it.ytex[m] = plan_ytex(p, m);
             it.tex[m] = plan_tex(p, m);
             it.gexp[m] = b->d_gexp + b->gexp_off[(size_t)s * kMaxM + m];
         }
-        it.tiles_u = (it.g.U + b->tile_u - 1) / b->tile_u;
-        it.tiles_v = (it.g.V + b->tile_v - 1) / b->tile_v;
+        it.tiles_u = (it.g.U + b->tile_u[kind] - 1) / b->tile_u[kind];
+        it.tiles_v = (it.g.V + b->tile_v[kind] - 1) / b->tile_v[kind];
         it.unit0 = unit0;
         it.units = units;
     }
@@ -533,7 +575,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         if (plan_device(plans[i]) != dev) return bfail(CTFP_INVALID_ARG, "plans must share one device");
         if (!batchable(plans[i]))
             return bfail(CTFP_UNSUPPORTED,
-                         "batched items need the layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
+                         "batched items need the axis or layered sampler (or CTFP_INTERP_TEXTURE) and no focal spot");
         if (plan_energies(plans[i]) < 1) return bfail(CTFP_NOT_READY, "spectral tables not set for an item");
     }
     DevScope ds(dev);
@@ -550,8 +592,10 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         const GeomParams& g = plan_geom(plans[i]);
         cost[(size_t)i] = (double)g.U * g.V * g.P * g.K * plan_materials(plans[i]);
     }
-    auto gkey = [&](int i) { return plan_materials(plans[i]) * 4 + plan_interp(plans[i]); };
-    std::vector<double> gcost(32, 0.0);
+    auto gkey = [&](int i) {
+        return (plan_materials(plans[i]) * 4 + plan_interp(plans[i])) * 2 + (uses_axis(plans[i]) ? 1 : 0);
+    };
+    std::vector<double> gcost(64, 0.0);
     for (int i = 0; i < n_items; i++) gcost[(size_t)gkey(i)] += cost[(size_t)i];
     b->order.resize((size_t)n_items);
     std::iota(b->order.begin(), b->order.end(), 0);
@@ -561,6 +605,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         return cost[(size_t)x] > cost[(size_t)y];
     });
     b->items.resize((size_t)n_items);
+    b->item_axis.resize((size_t)n_items);
     b->vox0.resize((size_t)n_items);
     b->gexp_off.assign((size_t)n_items * kMaxM, 0);
     long long unit = 0, vox = 0;
@@ -571,8 +616,11 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         ItemDesc& it = b->items[(size_t)s];
         it.M = plan_materials(p);
         it.interp = plan_interp(p);
-        if (b->groups.empty() || b->groups.back().M != it.M || b->groups.back().interp != it.interp)
-            b->groups.push_back({it.M, it.interp, s, 0, unit, unit, {0, 0}});
+        const int ax = uses_axis(p) ? 1 : 0;
+        b->item_axis[(size_t)s] = ax != 0;
+        if (b->groups.empty() || b->groups.back().M != it.M || b->groups.back().interp != it.interp ||
+            b->groups.back().axis != ax)
+            b->groups.push_back({it.M, it.interp, ax, s, 0, unit, unit, {0, 0}});
         b->groups.back().count++;
         b->vox0[(size_t)s] = vox;
         vox += (long long)g.nx * g.ny * g.nz;
@@ -581,7 +629,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
             gexp += expanded_elems(g);
         }
     }
-    layout_units(b);
+    layout_units(b, 0);
     b->total_vox = vox;
     b->gexp_elems = gexp;
     cudaError_t e = cudaMalloc(&b->d_items[0], sizeof(ItemDesc) * (size_t)n_items);
@@ -597,7 +645,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
     for (ctfp_batch::Group& G : b->groups) {
         for (int k = 0; k < 2 && e == cudaSuccess; k++) {
             int per = 0;
-            KernelFn fn = k ? kernel_for<true>(G.M, G.interp) : kernel_for<false>(G.M, G.interp);
+            KernelFn fn = k ? kernel_for<true>(G.M, G.interp, G.axis) : kernel_for<false>(G.M, G.interp, G.axis);
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, 0);
             G.grid[k] = std::max(1, per) * std::max(1, nsm);
         }
@@ -607,7 +655,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         return bfail(e == cudaErrorMemoryAllocation ? CTFP_OOM : CTFP_CUDA_ERROR,
                      std::string("ctfp_batch_create: ") + cudaGetErrorString(e));
     }
-    ctfp_status rs = fill_items(b);
+    ctfp_status rs = fill_items(b, 0);
     if (rs != CTFP_OK) {
         ctfp_batch_destroy(b);
         return rs;
@@ -638,7 +686,7 @@ ctfp_status ctfp_batch_forward(ctfp_batch* b, const float* const* const* volumes
     if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
     if (!volumes || !I) return bfail(CTFP_INVALID_ARG, "volumes and I are required");
     DevScope ds(b->device);
-    ctfp_status rs = fill_items(b);
+    ctfp_status rs = fill_items(b, 0);
     if (rs != CTFP_OK) return rs;
     std::vector<const float*> vols;
     for (int s = 0; s < b->n; s++) {
@@ -660,7 +708,7 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* b, const float* const* const*
     if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
     if (!volumes || !I_target || !g_volumes) return bfail(CTFP_INVALID_ARG, "volumes, I_target, g_volumes are required");
     DevScope ds(b->device);
-    ctfp_status rs = fill_items(b);
+    ctfp_status rs = fill_items(b, 1);
     if (rs != CTFP_OK) return rs;
     std::vector<const float*> vols;
     for (int s = 0; s < b->n; s++) {
@@ -692,9 +740,9 @@ ctfp_status ctfp_batch_set_shape(ctfp_batch* b, int32_t tile_u, int32_t tile_v)
         if (G.exec) cudaGraphExecDestroy(G.exec);
         G.exec = nullptr;
     }
-    b->tile_u = tile_u;
-    b->tile_v = tile_v;
-    layout_units(b);
+    b->tile_u[0] = b->tile_u[1] = tile_u;
+    b->tile_v[0] = b->tile_v[1] = tile_v;
+    layout_units(b, 0);
     return CTFP_OK;
 }
 
@@ -737,48 +785,74 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     BATCH_CUDA(cudaEventCreate(&e1));
     freer.c = e1;
     static const int shapes[][2] = {{8, 8}, {16, 4}, {4, 16}, {32, 2}, {2, 32}};
-    const int keep[2] = {b->tile_u, b->tile_v};
-    int best = -1;
-    float best_ms = 0.f;
-    for (int c = 0; c < (int)(sizeof(shapes) / sizeof(shapes[0])); c++) {
-        b->tile_u = shapes[c][0];
-        b->tile_v = shapes[c][1];
-        layout_units(b);
-        ctfp_status rs = fill_items(b);
-        if (rs != CTFP_OK) return rs;
-        for (int s = 0; s < b->n; s++) {
-            ItemDesc& it = b->items[(size_t)s];
-            it.I_target = I_target[b->order[(size_t)s]];
-            it.loss = loss + b->order[(size_t)s];
-        }
-        BATCH_CUDA(cudaStreamSynchronize(st));
-        BATCH_CUDA(cudaMemcpy(b->d_items[1], b->items.data(), sizeof(ItemDesc) * (size_t)b->n, cudaMemcpyHostToDevice));
-        rs = record(b, true, vols, loss, st, 8);  // warm-up
-        if (rs != CTFP_OK) return rs;
-        BATCH_CUDA(cudaEventRecord(e0, st));
-        rs = record(b, true, vols, loss, st, 8);
-        if (rs != CTFP_OK) return rs;
-        BATCH_CUDA(cudaEventRecord(e1, st));
-        BATCH_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (best < 0 || ms < best_ms) {
-            best = c;
-            best_ms = ms;
+    const int nshapes = (int)(sizeof(shapes) / sizeof(shapes[0]));
+    int best[2] = {-1, -1};
+    float best_ms[2] = {0.f, 0.f};
+    // each kind of call on its own kernel: the forward, then the fused
+    // forward + adjoint
+    for (int kind = 0; kind < 2; kind++) {
+        for (int c = 0; c < nshapes; c++) {
+            b->tile_u[kind] = shapes[c][0];
+            b->tile_v[kind] = shapes[c][1];
+            layout_units(b, kind);
+            ctfp_status rs = fill_items(b, kind);
+            if (rs != CTFP_OK) return rs;
+            for (int s = 0; s < b->n; s++) {
+                ItemDesc& it = b->items[(size_t)s];
+                it.I_target = I_target[b->order[(size_t)s]];
+                it.loss = kind ? loss + b->order[(size_t)s] : nullptr;
+                it.I = nullptr;  // the forward's outputs go nowhere while tuning
+                it.IAbs = nullptr;
+                it.L = nullptr;
+            }
+            BATCH_CUDA(cudaStreamSynchronize(st));
+            BATCH_CUDA(cudaMemcpy(b->d_items[kind], b->items.data(), sizeof(ItemDesc) * (size_t)b->n,
+                                  cudaMemcpyHostToDevice));
+            rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);  // warm-up
+            if (rs != CTFP_OK) return rs;
+            BATCH_CUDA(cudaEventRecord(e0, st));
+            rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);
+            if (rs != CTFP_OK) return rs;
+            BATCH_CUDA(cudaEventRecord(e1, st));
+            BATCH_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (best[kind] < 0 || ms < best_ms[kind]) {
+                best[kind] = c;
+                best_ms[kind] = ms;
+            }
         }
     }
-    b->tile_u = keep[0];
-    b->tile_v = keep[1];
-    const ctfp_status rs = ctfp_batch_set_shape(b, shapes[best][0], shapes[best][1]);
-    if (rs != CTFP_OK) return rs;
+    // graphs recorded with the old queues may still be running
+    BATCH_CUDA(cudaDeviceSynchronize());
+    for (ctfp_batch::Graph& G : b->graph) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+    }
+    for (int kind = 0; kind < 2; kind++) {
+        b->tile_u[kind] = shapes[best[kind]][0];
+        b->tile_v[kind] = shapes[best[kind]][1];
+    }
+    layout_units(b, 0);
     if (out) {
-        out->tile_u = shapes[best][0];
-        out->tile_v = shapes[best][1];
+        out->tile_u = shapes[best[1]][0];
+        out->tile_v = shapes[best[1]][1];
         out->views_per_cta = 1;
         out->min_ctas_per_sm = 0;
-        out->ms = best_ms;
+        out->ms = best_ms[1];
         out->from_cache = 0;
     }
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_batch_get_shapes(const ctfp_batch* b, int32_t* fwd_tile_u, int32_t* fwd_tile_v,
+                                  int32_t* adj_tile_u, int32_t* adj_tile_v)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (fwd_tile_u) *fwd_tile_u = b->tile_u[0];
+    if (fwd_tile_v) *fwd_tile_v = b->tile_v[0];
+    if (adj_tile_u) *adj_tile_u = b->tile_u[1];
+    if (adj_tile_v) *adj_tile_v = b->tile_v[1];
     return CTFP_OK;
 }
 

@@ -78,10 +78,17 @@ cudaError_t launch_count_support(const GeomParams& g, unsigned long long* out, c
 cudaError_t launch_shift_views(const float* in, float* out, const GeomParams& g, int M, int interp, int view0,
                                int n_views, cudaStream_t st);
 // SAMPLER_AXIS: writes one volume [nz][ny][nx] into its x-layered copy
-// (surface xs: layer x, texel (y, z)) and its y-layered copy (ys: layer y,
-// texel (x, z)).
+// (surface xs: texture layer x + 1, texel (y, z)) and its y-layered copy (ys:
+// texture layer y + 1, texel (x, z)).
 cudaError_t launch_axis_fill(const float* vol, int nx, int ny, int nz, cudaSurfaceObject_t xs, cudaSurfaceObject_t ys,
                              cudaStream_t st);
+// The axis march's texture quad-gathers over every view of a problem, with the
+// launch shape's tile and lane layout: out[0] += quads, out[1] += samples.
+cudaError_t launch_axis_gather_count(const GeomParams& g, int interp, const LaunchShape& ls, unsigned long long* out,
+                                     cudaStream_t st);
+// Zeros the pad layers (0 and the last) of both copies; once per array.
+cudaError_t launch_axis_zero_pads(int nx, int ny, int nz, cudaSurfaceObject_t xs, cudaSurfaceObject_t ys,
+                                  cudaStream_t st);
 // Fills occ [occ_dim(nz)][occ_dim(ny)][occ_dim(nx)] from the M volumes
 // (vol: host array of M device pointers; occ is zeroed first).
 cudaError_t launch_occupancy(const float* const* vol, int M, int nx, int ny, int nz, uint8_t* occ, cudaStream_t st);

@@ -318,6 +318,13 @@ class Projector:
              self._vol_ptrs(grads, "gradient"), _stream(stream))
         return grads
 
+    def axis_gather_count(self) -> float:
+        """ctfp_axis_gather_count: texture quad-gathers per voxel-sample of the
+        axis sampler's march (0.5 = both gathers of every sample in full warps)."""
+        r = C.c_double()
+        call("ctfp_axis_gather_count", self._h, C.byref(r))
+        return float(r.value)
+
     def count_support_samples(self) -> int:
         n = C.c_int64()
         call("ctfp_count_support_samples", self._h, C.byref(n))
@@ -352,13 +359,23 @@ class Batch:
         call("ctfp_batch_set_shape", self._h, tile_u, tile_v)
 
     def autotune(self, volumes: Sequence[Sequence], targets: Sequence, stream=None) -> dict:
-        """ctfp_batch_autotune: times the fused kernels with candidate unit shapes, keeps the fastest."""
+        """ctfp_batch_autotune: times the forward and the fused kernels with
+        candidate unit shapes and keeps the fastest of each; returns the fused
+        kernel's tile (tile_u, tile_v, ms) and the forward's (fwd_tile_u, fwd_tile_v)."""
         self._keep = []
         vt = self._vol_table(volumes)
         T = self._item_ptrs(targets, 1, "target")
         r = capi.LaunchShape()
         call("ctfp_batch_autotune", self._h, vt, T, C.byref(r), _stream(stream))
-        return {"tile_u": r.tile_u, "tile_v": r.tile_v, "ms": r.ms}
+        sh = self.shapes()
+        return {"tile_u": r.tile_u, "tile_v": r.tile_v, "ms": r.ms, "fwd_tile_u": sh["fwd"][0],
+                "fwd_tile_v": sh["fwd"][1]}
+
+    def shapes(self) -> dict:
+        """ctfp_batch_get_shapes: the work-unit ray tiles of the two kinds of call."""
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        call("ctfp_batch_get_shapes", self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return {"fwd": (int(a.value), int(b.value)), "fwd_adjoint": (int(c.value), int(d.value))}
 
     def info(self) -> dict:
         u, g0, g1 = C.c_int64(), C.c_int32(), C.c_int32()

@@ -86,8 +86,8 @@ typedef enum ctfp_sampler {
     /* the caller's linear volumes through L1 (8 loads per corner set) */
     CTFP_SAMPLER_GLOBAL = 1,
     /* plan-owned layered 2D textures, one layer per z slice: two texture
-     * gathers (tld4) return the 8 corners; weights stay in software.  Default;
-     * needs pNumZ <= 2048. */
+     * gathers (tld4) return the 8 corners; weights stay in software.  The
+     * default where the axis sampler does not fit; needs pNumZ <= 2048. */
     CTFP_SAMPLER_LAYERED = 2,
     /* the caller's linear volumes staged per ray bundle in shared memory: each
      * CTA (8 x 16 rays, one view at a time) copies the voxel box its rays cross
@@ -102,9 +102,9 @@ typedef enum ctfp_sampler {
      * central ray runs closest to, so consecutive samples of a ray mostly keep
      * their 2x2 in-layer footprint or move it one layer on; the gathers a ray
      * already holds are kept in registers and only the missing layers are
-     * fetched (on poly_grid_256 about a third of the two gathers per sample of
-     * CTFP_SAMPLER_LAYERED).  Results are bitwise those of the layered sampler.
-     * Needs pNumX, pNumY <= 2048 and pNumZ <= 32768. */
+     * fetched.  Results agree with the layered sampler to FP32 rounding (the
+     * layer axis is interpolated last).  The default; needs pNumX, pNumY <= 2046
+     * and pNumZ <= 32768 (else the layered sampler, else the global one). */
     CTFP_SAMPLER_AXIS = 4
 } ctfp_sampler;
 
@@ -140,8 +140,9 @@ ctfp_status ctfp_plan_set_interp(ctfp_plan* plan, int32_t interp);
 ctfp_status ctfp_plan_set_sampler(ctfp_plan* plan, int32_t sampler);
 /* Ray-tile shape of the march kernels: tile_u x tile_v pixels per CTA (a
  * multiple of 32 threads, at most 256), views_per_cta views marched by each
- * CTA for its tile, and min_ctas_per_sm (2, 3 or 4), the residency the forward
- * march is compiled for (its register cap: 65536 / (256 * min_ctas_per_sm)).
+ * CTA for its tile, and min_ctas_per_sm (2, 3, 4, or 5 for the axis sampler;
+ * other samplers run 5 as 4), the residency the forward march is compiled for
+ * (its register cap: 65536 / (256 * min_ctas_per_sm)).
  * Set by the autotuner; defaults 16 x 8 x 2 x 4. */
 ctfp_status ctfp_plan_set_launch_shape(ctfp_plan* plan, int32_t tile_u, int32_t tile_v, int32_t views_per_cta,
                                        int32_t min_ctas_per_sm);
@@ -308,8 +309,9 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * the plans' own texture arrays: do not run a batch and its plans
  * concurrently.
  *
- * Items use the layered sampler (the default) in CTFP_INTERP_TRILINEAR or
- * CTFP_INTERP_TEXEMU, or CTFP_INTERP_TEXTURE (hardware tex3D; its adjoint is the
+ * Items use the axis sampler (the default) or the layered one in
+ * CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU, or CTFP_INTERP_TEXTURE
+ * (hardware tex3D; its adjoint is the
  * transpose of the texture unit's weights, as ctfp_backward), have no focal
  * spot and have spectral tables set.  The batch keeps the
  * plans' pointers: destroy it before them.  Arrays indexed by item follow the
@@ -336,20 +338,26 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* co
 /* Work units in the queue, persistent grid sizes of the two kernels. */
 /* Ray tile of a work unit (one view): tile_u x tile_v rays, whose product must
  * be 64, the threads of a persistent CTA, with tile_u a power of two (default
- * 8 x 8).  Waits for the
- * device; the next call re-records its graph.  (A unit holds one view: a
- * runtime loop over several views cost the persistent kernels spills.) */
+ * 8 x 8), for both kinds of call.  Waits for the device; the next call
+ * re-records its graph.  (A unit holds one view: a runtime loop over several
+ * views cost the persistent kernels spills.) */
 ctfp_status ctfp_batch_set_shape(ctfp_batch* batch, int32_t tile_u, int32_t tile_v);
-/* Times the fused forward + loss + adjoint kernels with candidate ray tiles
- * (8 x 8, 16 x 4, 4 x 16, 32 x 2, 2 x 32) on the first eighth of every group's
- * work queue (its largest problems) and keeps the fastest.  Reads volumes and
- * I_target as ctfp_batch_forward_adjoint does and writes nothing the caller
- * owns; out (may be NULL) receives tile_u, tile_v, views_per_cta = 1 and ms.
+/* Times, for each kind of call on its own, the forward and the fused forward
+ * + loss + adjoint kernels with candidate ray tiles (8 x 8, 16 x 4, 4 x 16,
+ * 32 x 2, 2 x 32) on the first eighth of every group's work queue (its
+ * largest problems) and keeps the fastest tile of each kind.  Reads volumes
+ * and I_target as ctfp_batch_forward_adjoint does and writes nothing the
+ * caller owns; out (may be NULL) receives the fused kernel's tile_u, tile_v,
+ * views_per_cta = 1 and ms (ctfp_batch_get_shapes returns both tiles).
  * Waits for the device. */
 ctfp_status ctfp_batch_autotune(ctfp_batch* batch, const float* const* const* volumes, const float* const* I_target,
                                 ctfp_launch_shape* out, void* stream);
 ctfp_status ctfp_batch_info(const ctfp_batch* batch, int64_t* total_units, int32_t* grid_forward,
                             int32_t* grid_adjoint);
+/* The work-unit ray tiles of the forward and of the fused forward + adjoint
+ * calls (any pointer may be NULL). */
+ctfp_status ctfp_batch_get_shapes(const ctfp_batch* batch, int32_t* fwd_tile_u, int32_t* fwd_tile_v,
+                                  int32_t* adj_tile_u, int32_t* adj_tile_v);
 
 /* ---- view ranges (sharding one object's views across GPUs) -----------------
  * No counterpart in the reference.  The forward and the adjoint over views
@@ -459,6 +467,18 @@ ctfp_status ctfp_sample_volume(const float* volume, int64_t nx, int64_t ny, int6
 /* Exact number of (ray, sample) pairs whose trilinear footprint touches the
  * volume, i.e. the samples the march evaluates (others contribute exactly 0). */
 ctfp_status ctfp_count_support_samples(ctfp_plan* plan, int64_t* out);
+
+/* The texture work of the axis sampler's march on this plan's geometry with
+ * its launch shape: every view's rays are stepped as the march steps them
+ * and, per iteration of a warp and per gather slot, the 4-lane quads with a
+ * lane that fetches are counted (the texture unit spends its time per active
+ * quad).  quad_gathers_per_sample = quads counted / (ray, sample) pairs
+ * evaluated, per material.  Fetching both slots on every sample in full warps
+ * (as the layered sampler's two gathers do) gives 0.5 (16 quads per 32
+ * samples), so the axis march's texture roof is ctfp_sampler_peak
+ * (CTFP_SAMPLER_LAYERED) x 0.5 / quad_gathers_per_sample voxel-samples/s.
+ * Does not depend on the volumes.  No counterpart in the reference. */
+ctfp_status ctfp_axis_gather_count(ctfp_plan* plan, double* quad_gathers_per_sample);
 
 /* Message of the last error on the calling thread ("" if none). */
 const char* ctfp_last_error_string(void);

@@ -190,10 +190,29 @@ def test_batch_autotune_keeps_results(cuda_ok):
     grads = [[torch.zeros_like(v) for v in it[1]] for it in items]
     shape = b.autotune([it[1] for it in items], targets)
     assert shape["tile_u"] * shape["tile_v"] == 64 and shape["ms"] > 0
+    sh = b.shapes()  # the forward's and the fused kernel's tiles, tuned apart
+    assert sh["fwd_adjoint"] == (shape["tile_u"], shape["tile_v"])
+    assert sh["fwd"][0] * sh["fwd"][1] == 64 and sh["fwd"] == (shape["fwd_tile_u"], shape["fwd_tile_v"])
     assert all(float(g.abs().max()) == 0.0 for gk in grads for g in gk)
     res = b.forward_adjoint([it[1] for it in items], targets, grads=grads)
     torch.cuda.synchronize()
     for k, (pr, _, _) in enumerate(items):
         for m in range(pr.M):
             assert rel(res["grads"][k][m], ref_grads[k][m]) < 1e-4
+    b.close()
+
+
+def test_batch_mixed_samplers_equal_plain_calls(cuda_ok):
+    # items on the axis sampler (the default) and on the z-layered one run in
+    # groups of their own, each equal to its plain calls
+    items = make_items(ITEMS[:4])
+    items[0][0].set_sampler("layered")
+    items[2][0].set_sampler("layered")
+    b = Batch([it[0] for it in items])
+    outs = b.forward([it[1] for it in items], want_L=True)
+    torch.cuda.synchronize()
+    for (pr, vols, _), o in zip(items, outs):
+        ref = pr.forward(vols, want_L=True)
+        torch.cuda.synchronize()
+        assert rel(o["I"], ref["I"]) < 2e-6 and rel(o["L"], ref["L"]) < 1e-6
     b.close()

@@ -347,6 +347,7 @@ def test_brick_sampler_equals_layered(cuda_ok, mode, pitch, n, staging, monkeypa
     S, mu, G, D = spectral_setup(d, 3, 6, 2)
     with Projector(d, 3, mode) as pr:
         pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_sampler("layered")
         a = pr.forward(to_dev(vols), want_L=True)
         pr.set_sampler("brick")
         b = pr.forward(to_dev(vols), want_L=True)
@@ -366,6 +367,7 @@ def test_brick_tma_wait_that_runs_out(cuda_ok, monkeypatch):
     S, mu, G, D = spectral_setup(d, 2, 5, 3)
     with Projector(d, 2, "trilinear") as pr:
         pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
+        pr.set_sampler("layered")
         a = pr.forward(to_dev(vols), want_L=True)
         pr.set_sampler("brick")
         monkeypatch.setenv("CTFP_WAIT_LIMIT", "0")
@@ -479,9 +481,10 @@ def test_focal_spot_zero_offsets_equal_plain_forward(cuda_ok, mode):
     assert rel_err(c["I"].cpu().numpy(), a["I"][1:3].cpu().numpy()) < 1e-6
 
 
-def test_deep_volume_falls_back_to_global_sampler(cuda_ok):
-    # layered textures hold at most 2048 layers: a deeper volume is marched
-    # through the global sampler, and asking for the layered one is refused
+def test_deep_volume_default_sampler_and_layered_refused(cuda_ok):
+    # layered textures hold at most 2048 layers: a volume 2050 slices deep is
+    # marched by the default axis sampler (layers along x and y), and asking
+    # for the z-layered one is refused
     from ct_forward_projection_b200._capi import CtfpError, CTFP_UNSUPPORTED
     d = small_geometry(n=(6, 5, 2050), views=2, U=7, V=9, length=6.0, pitch=2.0)
     vols = random_volumes(d, 1, 3)
@@ -490,6 +493,16 @@ def test_deep_volume_falls_back_to_global_sampler(cuda_ok):
         with pytest.raises(CtfpError) as e:
             pr.set_sampler("layered")
         assert e.value.status == CTFP_UNSUPPORTED
+    assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
+
+
+def test_wide_volume_falls_back_to_layered_sampler(cuda_ok):
+    # the axis sampler's copies hold at most 2046 voxel layers along x and y:
+    # a volume 2050 voxels wide is marched by the z-layered sampler
+    d = small_geometry(n=(2050, 4, 3), views=3, U=9, V=5, length=20.0, pitch=2.0)
+    vols = random_volumes(d, 1, 4)
+    with Projector(d, 1, "trilinear") as pr:
+        L = pr.line_integrals(to_dev(vols)).cpu().numpy().reshape(-1, 1)
     assert rel_err_scaled(L, O.line_integrals(d, vols)) < RTOL_TRI
 
 
@@ -507,8 +520,9 @@ AXIS_GEOMS = [
 @pytest.mark.parametrize("gi", range(len(AXIS_GEOMS)))
 @pytest.mark.parametrize("M", [1, 2, 3, 4])
 def test_axis_sampler_equals_layered(cuda_ok, mode, gi, M):
-    """The axis sampler reads the same voxel values with the same weights in
-    the same order as the layered sampler: outputs are bitwise equal."""
+    """The axis sampler reads the same voxel values with the same weights as
+    the layered sampler, interpolating the layer axis last: outputs agree to
+    FP32 rounding (and each matches the oracle in the parity tests)."""
     d = small_geometry(**AXIS_GEOMS[gi])
     vols = random_volumes(d, M, 500 + 10 * gi + M)
     S, mu, G, D = spectral_setup(d, M, 7, 3 + gi)
@@ -519,22 +533,24 @@ def test_axis_sampler_equals_layered(cuda_ok, mode, gi, M):
         pr.set_sampler("axis")
         b = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
-    for k in ("L", "I", "IAbsorb", "I0"):
-        assert torch.equal(a[k], b[k]), k
+    assert torch.equal(a["I0"], b["I0"])
+    for k in ("I", "IAbsorb"):
+        assert rel_err(b[k].cpu().numpy(), a[k].cpu().numpy()) < 1e-6, k
+    assert rel_err_scaled(b["L"].cpu().numpy(), a["L"].cpu().numpy()) < 1e-6
 
 
 @pytest.mark.parametrize("mode", ["trilinear", "texemu"])
 @pytest.mark.parametrize("shape", [(16, 16, 1, 3), (32, 8, 2, 4), (8, 32, 4, 2), (16, 4, 1, 3), (64, 2, 1, 3)])
 def test_axis_sampler_launch_shapes(cuda_ok, mode, shape):
     """Every launch shape gives the same outputs (tiles whose height is not a
-    multiple of 4 run as 16 x 16)."""
+    multiple of 4 run as 16 x 16): bitwise, since each ray is marched alone."""
     d = small_geometry(n=(20, 24, 16), views=9, U=37, V=23)
     vols = random_volumes(d, 2, 77)
     S, mu, G, D = spectral_setup(d, 2, 5, 8)
     with Projector(d, 2, mode) as pr:
         pr.set_spectral_tables(S, mu, G, 2, D, 1000.0)
-        a = pr.forward(to_dev(vols), want_L=True)
         pr.set_sampler("axis")
+        a = pr.forward(to_dev(vols), want_L=True)
         pr.set_launch_shape(*shape)
         b = pr.forward(to_dev(vols), want_L=True)
         torch.cuda.synchronize()
@@ -566,3 +582,28 @@ def test_axis_sampler_limits(cuda_ok):
         with pytest.raises(CtfpError) as e:
             pr.set_sampler("axis")
         assert e.value.status == CTFP_UNSUPPORTED
+
+
+@pytest.mark.parametrize("gi", range(len(AXIS_GEOMS)))
+@pytest.mark.parametrize("mode", ["trilinear", "texemu"])
+def test_axis_gather_count_bounds(cuda_ok, gi, mode):
+    """The axis march's texture work per voxel-sample is positive and at most
+    both slots of every sample with one live lane per quad (2.0); it does not
+    depend on the volumes and is the same on every call."""
+    d = small_geometry(**AXIS_GEOMS[gi])
+    with Projector(d, 2, mode) as pr:
+        pr.set_sampler("axis")
+        g = pr.axis_gather_count()
+        assert pr.axis_gather_count() == g
+    assert 0.0 < g <= 2.0
+
+
+def test_axis_gather_count_reuse_on_a_fine_march(cuda_ok):
+    # a 64^3 volume sampled at half a voxel by a 128-column detector: most
+    # samples keep or advance their footprint, so fewer than 60 % of the
+    # two-gather work is fetched
+    d = small_geometry(n=64, views=12, U=128, V=32, length=64.0)
+    with Projector(d, 1, "trilinear") as pr:
+        pr.set_sampler("axis")
+        g = pr.axis_gather_count()
+    assert g < 0.3
