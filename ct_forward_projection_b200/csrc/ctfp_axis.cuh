@@ -136,7 +136,7 @@ __device__ __forceinline__ void march_ray_axis(const GeomParams& g, const cudaTe
         int e0, e1;
         bool n0, n1;
         hold.fetch(lc, a, b, e0, e1, n0, n1);
-        const float fa = (float)(a + 1), fb = (float)(b + 1);
+        const float fa = small_int_to_float(a + 1), fb = small_int_to_float(b + 1);
         if (n0) {
 #pragma unroll
             for (int m = 0; m < M; m++) q0[m] = gather_layer_cond(tx[m], e0 + 1, fa, fb);
@@ -227,6 +227,156 @@ __device__ __forceinline__ void count_ray_axis(const GeomParams& g, int p, int v
     samples = __reduce_add_sync(warp_mask, (unsigned)samples);
     out[0] = quads;
     out[1] = samples;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint accumulators, face-expanded along the march axis.  One float4 array
+// per material holds two blocks: the x-face block, cells (x, z + 1, y + 1) of
+// nx x (nz + 1) x (ny + 1), then the y-face block, cells (y, z + 1, x + 1) of
+// ny x (nz + 1) x (nx + 1).  Cell (layer l, in-layer base a, z base b) of a
+// block holds the contributions to the 2 x 2 face of layer l with lower corner
+// (a, b): components (a, b), (a + 1, b), (a, b + 1), (a + 1, b + 1).  Views
+// marched along x scatter into the x-face block, the others into the y-face
+// block; face_fold sums both blocks into each voxel.
+__host__ __device__ __forceinline__ size_t xface_elems(int nx, int ny, int nz)
+{
+    return (size_t)nx * (size_t)(nz + 1) * (size_t)(ny + 1);
+}
+__host__ __device__ __forceinline__ size_t face_elems(int nx, int ny, int nz)
+{
+    return xface_elems(nx, ny, nz) + (size_t)ny * (size_t)(nz + 1) * (size_t)(nx + 1);
+}
+template <int AX>
+__device__ __forceinline__ size_t face_index(int nx, int ny, int nz, int l, int a, int b)
+{
+    if (AX == 0) return ((size_t)l * (size_t)(nz + 1) + (size_t)(b + 1)) * (size_t)(ny + 1) + (size_t)(a + 1);
+    return xface_elems(nx, ny, nz) +
+           ((size_t)l * (size_t)(nz + 1) + (size_t)(b + 1)) * (size_t)(nx + 1) + (size_t)(a + 1);
+}
+
+// The gradient contribution of every face cell that touches voxel (x, y, z).
+__device__ __forceinline__ float face_fold(const float4* __restrict__ e, int nx, int ny, int nz, int x, int y, int z)
+{
+    // x faces of layer x: bases (y, z), (y - 1, z), (y, z - 1), (y - 1, z - 1)
+    const float4* ex = e + face_index<0>(nx, ny, nz, x, 0, 0) - (size_t)(ny + 1) - 1;  // the (a, b) = (-1, -1) cell
+    const size_t row = (size_t)(ny + 1);
+    const float sx = (ex[(size_t)(z + 1) * row + (y + 1)].x + ex[(size_t)(z + 1) * row + y].y) +
+                     (ex[(size_t)z * row + (y + 1)].z + ex[(size_t)z * row + y].w);
+    const float4* ey = e + face_index<1>(nx, ny, nz, y, 0, 0) - (size_t)(nx + 1) - 1;
+    const size_t rowy = (size_t)(nx + 1);
+    const float sy = (ey[(size_t)(z + 1) * rowy + (x + 1)].x + ey[(size_t)(z + 1) * rowy + x].y) +
+                     (ey[(size_t)z * rowy + (x + 1)].z + ey[(size_t)z * rowy + x].w);
+    return sx + sy;
+}
+
+// Adjoint of one ray's march, accumulated per face of the march axis (AX):
+// the face weights a sample gives its lower layer and its upper layer are
+// summed in slot 0 (the even layer of the pair) and slot 1 (the odd one), as
+// the forward holds its gathers; a slot is flushed -- one 16-byte vector
+// reduction per material, its sums times the ray's dLoss/dL_m -- when its
+// layer or the in-layer base changes, and at the end of the ray.  Consecutive
+// samples keep their base and advance a layer on every second sample or so,
+// so a slot collects two or three samples per flush.  Layers and bases outside
+// the volume touch no voxel and are not flushed.
+template <int M, int AX>
+struct AxisScatter {
+    int h0 = -1000000000, h1 = -1000000000, ca = 0, cb = 0;
+    float s0[4] = {0.f, 0.f, 0.f, 0.f}, s1[4] = {0.f, 0.f, 0.f, 0.f};
+
+    __device__ __forceinline__ void flush(float4* const* __restrict__ acc, int nx, int ny, int nz, int l,
+                                          const float* sv, const float* g) const
+    {
+        const int nl = AX == 0 ? nx : ny, na = AX == 0 ? ny : nx;
+        if ((unsigned)l >= (unsigned)nl || ca < -1 || ca >= na || cb < -1 || cb >= nz) return;
+        const size_t k = face_index<AX>(nx, ny, nz, l, ca, cb);
+#pragma unroll
+        for (int m = 0; m < M; m++) red_add_v4(acc[m] + k, sv[0] * g[m], sv[1] * g[m], sv[2] * g[m], sv[3] * g[m]);
+    }
+
+    // The sample with footprint c and its 8 transposed weights w[k]
+    // (k = dz*4 + dy*2 + dx).
+    __device__ __forceinline__ void add(float4* const* __restrict__ acc, int nx, int ny, int nz, const Corner& c,
+                                        const float* w, const float* g)
+    {
+        const int lc = AX == 0 ? c.ix : c.iy, a = AX == 0 ? c.iy : c.ix, b = c.iz;
+        const int par = lc & 1;
+        const int e0 = lc + par, e1 = lc + 1 - par;
+        const bool base = (a == ca) & (b == cb);
+        if (!(base & (h0 == e0))) {
+            flush(acc, nx, ny, nz, h0, s0, g);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s0[j] = 0.f;
+        }
+        if (!(base & (h1 == e1))) {
+            flush(acc, nx, ny, nz, h1, s1, g);
+#pragma unroll
+            for (int j = 0; j < 4; j++) s1[j] = 0.f;
+        }
+        h0 = e0;
+        h1 = e1;
+        ca = a;
+        cb = b;
+        constexpr int lb = AX == 0 ? 1 : 2;  // the layer bit of k
+        constexpr int ab = AX == 0 ? 2 : 1;  // the in-layer axis bit of k
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int k = (j & 2 ? 4 : 0) + (j & 1 ? ab : 0);
+            s0[j] += par ? w[k + lb] : w[k];
+            s1[j] += par ? w[k] : w[k + lb];
+        }
+    }
+
+    __device__ __forceinline__ void finish(float4* const* __restrict__ acc, int nx, int ny, int nz, const float* g)
+    {
+        flush(acc, nx, ny, nz, h0, s0, g);
+        flush(acc, nx, ny, nz, h1, s1, g);
+    }
+};
+
+// The 8 transposed weights of a footprint (k = dz*4 + dy*2 + dx): the
+// trilinear products, or the texture unit's weights (TEXEMU).
+template <int MODE>
+__device__ __forceinline__ void corner_weights(const Corner& c, float* w)
+{
+    if (MODE == INTERP_TEXEMU) {
+        texunit_weights(c.qx, c.qy, c.qz, w);
+    } else {
+        const float uy_uz = c.uy * c.uz, wy_uz = c.wy * c.uz, uy_wz = c.uy * c.wz, wy_wz = c.wy * c.wz;
+        w[0] = c.ux * uy_uz; w[1] = c.wx * uy_uz; w[2] = c.ux * wy_uz; w[3] = c.wx * wy_uz;
+        w[4] = c.ux * uy_wz; w[5] = c.wx * uy_wz; w[6] = c.ux * wy_wz; w[7] = c.wx * wy_wz;
+    }
+}
+
+// The adjoint scatter of one ray: the transposed weights of the march's
+// samples (FP64 coordinates for TRILINEAR, the reference's FP32 coordinates
+// and the texture unit's weights otherwise) into the face accumulators of the
+// view's march axis, scaled by g[m] = dLoss/dL_m times dx.
+template <int M, int MODE>
+__device__ __forceinline__ void scatter_ray_axis(const GeomParams& gp, float4* const* __restrict__ acc, int p, int v,
+                                                 int u, const float* g, bool axis_x)
+{
+    const RaySeg s = ray_segment(gp, p, v, u);
+    RayRef32 r;
+    if (MODE != INTERP_TRILINEAR) r = ray_ref32(gp, p, v, u);
+    double cx = fma((double)s.i0, s.bx, s.ax), cy = fma((double)s.i0, s.by, s.ay), cz = fma((double)s.i0, s.bz, s.az);
+    float w[8];
+    if (axis_x) {
+        AxisScatter<M, 0> run;
+        for (int i = s.i0; i < s.i1; i++) {
+            const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
+            corner_weights<MODE>(c, w);
+            run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+        }
+        run.finish(acc, gp.nx, gp.ny, gp.nz, g);
+    } else {
+        AxisScatter<M, 1> run;
+        for (int i = s.i0; i < s.i1; i++) {
+            const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
+            corner_weights<MODE>(c, w);
+            run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+        }
+        run.finish(acc, gp.nx, gp.ny, gp.nz, g);
+    }
 }
 
 // Whether view p reads the x-layered copies: its central ray (direction

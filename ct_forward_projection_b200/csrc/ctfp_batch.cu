@@ -148,14 +148,7 @@ __device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s,
     for (int m = 0; m < M; m++) L[m] = it.g.dx * (acc[m] - cmp[m]);
 }
 
-template <int M, int MODE>
-__device__ __forceinline__ void batch_scatter(const ItemDesc& it, const RaySeg& s, const RayRef32& r, const float* g)
-{
-    ScatterRun<M> run;
-    for (int i = s.i0; i < s.i1; i++)
-        run.template add<MODE>(it.gexp, it.g.nx, it.g.ny, it.g.nz, batch_corner<MODE>(it, s, r, i), g);
-    run.flush(it.gexp, it.g.nx, it.g.ny, it.g.nz, g);
-}
+
 
 // One ray.  ADJOINT: the fused forward + loss + adjoint; returns the ray's
 // loss term.
@@ -170,34 +163,22 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     if (MODE != INTERP_TRILINEAR) r = ray_ref32(it.g, p, v, u);
     float L[M];
     batch_march<M, MODE, AXIS>(it, s, r, p, v, u, L);
-    float sI = 0.f, cI = 0.f, sA = 0.f, cA = 0.f, S[M];
-#pragma unroll
-    for (int m = 0; m < M; m++) S[m] = 0.f;
-    for (int e = 0; e < it.E; e++) {
-        float att = 0.f;
-#pragma unroll
-        for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
-        const float w = __ldg(it.W + (int64_t)e * npix + pix);
-        float ex, om;
-        transmit(att, ex, om);
-        const float Ie = w * ex;
-        kahan_add(sI, cI, Ie);
-        if (!ADJOINT) kahan_add(sA, cA, w * om);
-        if (ADJOINT) {
-#pragma unroll
-            for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
-        }
-    }
-    const float I = sI - cI;
-    if (it.I) it.I[ray] = I;
+    // the plain forward's epilogue (spectral / spectral_adjoint), so the
+    // batch's I equals ctfp_forward's for the same path integrals
     if (!ADJOINT) {
-        if (it.IAbs) it.IAbs[ray] = sA - cA;
+        float I, A;
+        spectral<M>(s_mu, it.E, it.W, pix, npix, L, I, A);
+        if (it.I) it.I[ray] = I;
+        if (it.IAbs) it.IAbs[ray] = A;
         if (it.L) {
 #pragma unroll
             for (int m = 0; m < M; m++) it.L[ray * M + m] = L[m];
         }
         return 0.f;
     }
+    float I, S[M];
+    spectral_adjoint<M>(s_mu, it.E, it.W, pix, npix, L, I, S);
+    if (it.I) it.I[ray] = I;
     // loss (log I - log T)^2: dLoss/dI = 2 (log I - log T) / I, dI/dL_m = -S_m
     if (!(I > 0.f)) return 0.f;
     const float res = logf(I) - logf(it.I_target[ray]);
@@ -211,7 +192,9 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     }
     // TEXTURE: the transpose of the texture unit's weights, which the
     // emulation reproduces exactly (as ctfp_backward does for such a plan)
-    if (any) batch_scatter<M, MODE == INTERP_TEXTURE ? INTERP_TEXEMU : MODE>(it, s, r, g);
+    if (any)
+        scatter_ray_axis<M, MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(it.g, it.gexp, p, v, u, g,
+                                                                                          axis_is_x(it.g, p));
     return res * res;
 }
 
@@ -309,14 +292,9 @@ __global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long
         }
         const ItemDesc& it = items[lo];
         const long long k = t - vox0[lo];
-        const int nx = it.g.nx, ny = it.g.ny;
+        const int nx = it.g.nx, ny = it.g.ny, nz = it.g.nz;
         const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((long long)nx * ny));
-        const size_t a = exp_index(nx, ny, x, y, z), b = exp_index(nx, ny, x - 1, y, z);
-        const size_t c = exp_index(nx, ny, x, y - 1, z), d = exp_index(nx, ny, x - 1, y - 1, z);
-        for (int m = 0; m < it.M; m++) {
-            const float4* e = it.gexp[m];
-            it.gvol[m][k] += (e[a].x + e[b].y) + (e[c].z + e[d].w);
-        }
+        for (int m = 0; m < it.M; m++) it.gvol[m][k] += face_fold(it.gexp[m], nx, ny, nz, x, y, z);
     }
 }
 

@@ -258,13 +258,24 @@ __device__ __forceinline__ Corner corner_tex(float3 x)
 // u = 1 - f, each rounded once from FP64 to FP32.  1 - f is exact in FP64 for
 // f >= 1/2 (and within 2^-53 of the true value, near 1, otherwise), so both
 // weights keep their FP32 relative accuracy however close to 0 either is.
+// The integer part comes from the floored double through the FP64 adder:
+// adding 1.5 * 2^52 leaves an integer-valued double in [-2^31, 2^31) as the low
+// word of the sum's significand (two's complement), which saves the two
+// conversions an int round trip costs.
 __device__ __forceinline__ int axis_weights(double x, float& w, float& u)
 {
-    const int b = __double2int_rd(x);
-    const double f = x - (double)b;
+    const double fl = floor(x);
+    const double f = x - fl;
     w = __double2float_rn(f);
     u = __double2float_rn(1.0 - f);
-    return b;
+    return __double2loint(fl + 6755399441055744.0);
+}
+
+// (float)n for -3 <= n < 2^23 - 3 without a conversion instruction: the bits
+// of 2^23 + (n + 3) as a float, minus 2^23 + 3 (exact).
+__device__ __forceinline__ float small_int_to_float(int n)
+{
+    return __int_as_float(0x4B000000 | (n + 3)) - 8388611.0f;
 }
 
 // Footprint at the FP64 coordinate (cx, cy, cz).  TRILINEAR: exact fraction
@@ -279,7 +290,7 @@ __device__ __forceinline__ Corner corner_of(double cx, double cy, double cz)
         c.ix = axis_weights(cx, c.wx, c.ux);
         c.iy = axis_weights(cy, c.wy, c.uy);
         c.iz = axis_weights(cz, c.wz, c.uz);
-        c.tx = (float)(c.ix + 1); c.ty = (float)(c.iy + 1);
+        c.tx = small_int_to_float(c.ix + 1); c.ty = small_int_to_float(c.iy + 1);
     } else {
         const int X = tex_fixed((float)(cx + 0.5)), Y = tex_fixed((float)(cy + 0.5)), Z = tex_fixed((float)(cz + 0.5));
         c.ix = X >> 8; c.iy = Y >> 8; c.iz = Z >> 8;
@@ -395,69 +406,13 @@ __device__ __forceinline__ void gather4_interp(const cudaTextureObject_t* ltex, 
     for (int m = 0; m < M; m++) out[m] = interp8<MODE>(c, v[m]);
 }
 
-// Corner-expanded adjoint accumulator.  The 8 transposed weights of a sample
-// go to two float4 cells, one per z slice of the footprint: cell (z, y, x)
-// holds the contributions of footprints with lower corner (x, y) in slice z to
-// the 4 voxels (x, y), (x+1, y), (x, y+1), (x+1, y+1).  Two 16-byte vector
-// reductions replace 8 scalar atomics; k_fold later sums the 4 cells that
-// touch each voxel.  Indices are offset by one in x and y and by one in z so
-// that footprints hanging over the volume's edge land in padding.
-__device__ __forceinline__ size_t exp_index(int nx, int ny, int x, int y, int z)
-{
-    return ((size_t)(z + 1) * (size_t)(ny + 1) + (size_t)(y + 1)) * (size_t)(nx + 1) + (size_t)(x + 1);
-}
-
+// One 16-byte vector reduction into global memory (the adjoint's accumulators).
 __device__ __forceinline__ void red_add_v4(float4* p, float a, float b, float c, float d)
 {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
                  : "memory");
 }
 
-// Adjoint contributions of consecutive samples that share a footprint.  A
-// ray's dLoss/dL_m (g[m]) is the same at every sample, so a run needs only
-// the sum of its samples' 8 weights; at the footprint's end (and at the end of
-// the ray) each material receives g[m] times that sum as one pair of vector
-// reductions: the same sums as one reduction pair per sample, in fewer L2
-// atomics, with 8 accumulators whatever the material count.
-template <int M>
-struct ScatterRun {
-    int ix = INT_MIN, iy = 0, iz = 0;
-    float a[8];
-    __device__ __forceinline__ void flush(float4* const* __restrict__ gexp, int nx, int ny, int nz, const float* g)
-    {
-        if (ix == INT_MIN) return;
-        if (ix < -1 || iy < -1 || iz < -1 || ix >= nx || iy >= ny || iz >= nz) return;
-        const size_t i0 = exp_index(nx, ny, ix, iy, iz);
-        const size_t i1 = exp_index(nx, ny, ix, iy, iz + 1);
-#pragma unroll
-        for (int m = 0; m < M; m++) {
-            red_add_v4(gexp[m] + i0, a[0] * g[m], a[1] * g[m], a[2] * g[m], a[3] * g[m]);
-            red_add_v4(gexp[m] + i1, a[4] * g[m], a[5] * g[m], a[6] * g[m], a[7] * g[m]);
-        }
-    }
-    template <int MODE>
-    __device__ __forceinline__ void add(float4* const* __restrict__ gexp, int nx, int ny, int nz, const Corner& c,
-                                        const float* g)
-    {
-        float w[8];
-        if (MODE == 1 /* INTERP_TEXEMU */) {
-            texunit_weights(c.qx, c.qy, c.qz, w);
-        } else {
-            const float ux = c.ux, uy = c.uy, uz = c.uz;
-            w[0] = ux * uy * uz; w[1] = c.wx * uy * uz; w[2] = ux * c.wy * uz; w[3] = c.wx * c.wy * uz;
-            w[4] = ux * uy * c.wz; w[5] = c.wx * uy * c.wz; w[6] = ux * c.wy * c.wz; w[7] = c.wx * c.wy * c.wz;
-        }
-        if (c.ix != ix || c.iy != iy || c.iz != iz) {
-            flush(gexp, nx, ny, nz, g);
-            ix = c.ix; iy = c.iy; iz = c.iz;
-#pragma unroll
-            for (int k = 0; k < 8; k++) a[k] = w[k];
-        } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) a[k] += w[k];
-        }
-    }
-};
 
 // exp(-a) and 1 - exp(-a), each to a few ulp relative.  For |a| < 1/4 the
 // absorbed fraction is the Taylor series 1 - exp(-a) = a (1 - a/2 + a^2/6 -
@@ -491,6 +446,77 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x)
     const float t = s + y;
     c = (t - s) - y;
     s = t;
+}
+
+// K2: I = sum_e W_e exp(-sum_m mu_em L_m), IAbs = sum_e W_e (1 - exp(...)).
+// The energy sums are split over 4 accumulators (energy e into e mod 4) and
+// combined pairwise: each takes about E / 4 positive terms, so the sum's
+// relative rounding error stays below (E / 4 + 2) ulp with one fused
+// multiply-add per term and output.
+template <int M>
+__device__ __forceinline__ void spectral_term(const float* s_mu, int e, const float* __restrict__ Wp, int64_t npix,
+                                              const float* L, float& sI, float& sA)
+{
+    float att = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
+    const float w = __ldg(Wp + (int64_t)e * npix);
+    float ex, om;
+    transmit(att, ex, om);
+    sI = fmaf(w, ex, sI);
+    sA = fmaf(w, om, sA);
+}
+
+template <int M>
+__device__ __forceinline__ void spectral(const float* s_mu, int E, const float* __restrict__ W, int64_t pix,
+                                         int64_t npix, const float* L, float& I, float& IAbs)
+{
+    float sI[4] = {0.f, 0.f, 0.f, 0.f}, sA[4] = {0.f, 0.f, 0.f, 0.f};
+    const float* Wp = W + pix;
+    int e = 0;
+    for (; e + 4 <= E; e += 4) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) spectral_term<M>(s_mu, e + k, Wp, npix, L, sI[k], sA[k]);
+    }
+    for (; e < E; e++) spectral_term<M>(s_mu, e, Wp, npix, L, sI[0], sA[0]);
+    I = (sI[0] + sI[1]) + (sI[2] + sI[3]);
+    IAbs = (sA[0] + sA[1]) + (sA[2] + sA[3]);
+}
+
+// The fused forward + loss + adjoint's epilogue: I as spectral() forms it
+// (the same terms in the same order, so the batch's I equals the plain
+// forward's), and S_m = sum_e mu_em W_e exp(-a_e), the derivative -dI/dL_m.
+template <int M>
+__device__ __forceinline__ void spectral_adjoint_term(const float* s_mu, int e, const float* __restrict__ Wp,
+                                                      int64_t npix, const float* L, float& sI, float* S)
+{
+    float att = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
+    const float w = __ldg(Wp + (int64_t)e * npix);
+    float ex, om;
+    transmit(att, ex, om);
+    sI = fmaf(w, ex, sI);
+    const float Ie = w * ex;
+#pragma unroll
+    for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
+}
+
+template <int M>
+__device__ __forceinline__ void spectral_adjoint(const float* s_mu, int E, const float* __restrict__ W, int64_t pix,
+                                                 int64_t npix, const float* L, float& I, float* S)
+{
+    float sI[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int m = 0; m < M; m++) S[m] = 0.f;
+    const float* Wp = W + pix;
+    int e = 0;
+    for (; e + 4 <= E; e += 4) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) spectral_adjoint_term<M>(s_mu, e + k, Wp, npix, L, sI[k], S);
+    }
+    for (; e < E; e++) spectral_adjoint_term<M>(s_mu, e, Wp, npix, L, sI[0], S);
+    I = (sI[0] + sI[1]) + (sI[2] + sI[3]);
 }
 
 }  // namespace ctfp

@@ -91,41 +91,6 @@ __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, 
     for (int m = 0; m < M; m++) L[m] = prm.g.dx * (acc[m] - cmp[m]);
 }
 
-// K2: I = sum_e W_e exp(-sum_m mu_em L_m), IAbs = sum_e W_e (1 - exp(...)).
-// The energy sums are split over 4 accumulators (energy e into e mod 4) and
-// combined pairwise: each takes about E / 4 positive terms, so the sum's
-// relative rounding error stays below (E / 4 + 2) ulp with one fused
-// multiply-add per term and output.
-template <int M>
-__device__ __forceinline__ void spectral_term(const float* s_mu, int e, const float* __restrict__ Wp, int64_t npix,
-                                              const float* L, float& sI, float& sA)
-{
-    float att = 0.f;
-#pragma unroll
-    for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
-    const float w = __ldg(Wp + (int64_t)e * npix);
-    float ex, om;
-    transmit(att, ex, om);
-    sI = fmaf(w, ex, sI);
-    sA = fmaf(w, om, sA);
-}
-
-template <int M>
-__device__ __forceinline__ void spectral(const float* s_mu, int E, const float* __restrict__ W, int64_t pix,
-                                         int64_t npix, const float* L, float& I, float& IAbs)
-{
-    float sI[4] = {0.f, 0.f, 0.f, 0.f}, sA[4] = {0.f, 0.f, 0.f, 0.f};
-    const float* Wp = W + pix;
-    int e = 0;
-    for (; e + 4 <= E; e += 4) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) spectral_term<M>(s_mu, e + k, Wp, npix, L, sI[k], sA[k]);
-    }
-    for (; e < E; e++) spectral_term<M>(s_mu, e, Wp, npix, L, sI[0], sA[0]);
-    I = (sI[0] + sI[1]) + (sI[2] + sI[3]);
-    IAbs = (sA[0] + sA[1]) + (sA[2] + sA[3]);
-}
-
 __device__ __forceinline__ void load_mu(float* s_mu, const float* mu, int n)
 {
     const int nt = blockDim.x * blockDim.y;
@@ -321,7 +286,7 @@ __global__ void __launch_bounds__(256) k_spectral_from_L(const MarchParams prm)
 // angle is small), so the accumulator cells they reduce into stay in L2; with
 // views outermost every view would sweep the whole accumulator through DRAM.
 template <int M, int MODE, bool FROM_GL>
-__global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
+__global__ void __launch_bounds__(256, 3) k_backward(const MarchParams prm)
 {
     extern __shared__ float s_mu[];
     if (!FROM_GL) load_mu(s_mu, prm.mu, prm.E * M);
@@ -345,11 +310,15 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
             load_L<M>(prm.Lin, ray, L);
 #pragma unroll
             for (int m = 0; m < M; m++) S[m] = 0.f;
+            // the spectral weights as the forward formed them (transmit, the
+            // same order), so S matches the fused kernels' exactly
             for (int e = 0; e < prm.E; e++) {
                 float att = 0.f;
 #pragma unroll
                 for (int m = 0; m < M; m++) att = fmaf(s_mu[e * M + m], L[m], att);
-                const float Ie = __ldg(prm.W + (int64_t)e * npix + pix) * expf(-att);
+                float ex, om;
+                transmit(att, ex, om);
+                const float Ie = __ldg(prm.W + (int64_t)e * npix + pix) * ex;
 #pragma unroll
                 for (int m = 0; m < M; m++) S[m] = fmaf(s_mu[e * M + m], Ie, S[m]);
             }
@@ -361,28 +330,15 @@ __global__ void __launch_bounds__(256) k_backward(const MarchParams prm)
 #pragma unroll
         for (int m = 0; m < M; m++) any |= (g[m] != 0.f);
         if (!any) continue;
-        const RaySeg s = ray_segment(prm.g, p, v, u);
-        ScatterRun<M> run;
-        if (MODE == INTERP_TRILINEAR) {
-            for (int i = s.i0; i < s.i1; i++) {
-                const double t = (double)i;
-                const Corner c = corner_of<INTERP_TRILINEAR>(fma(t, s.bx, s.ax), fma(t, s.by, s.ay), fma(t, s.bz, s.az));
-                run.template add<INTERP_TRILINEAR>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, c, g);
-            }
-        } else {
-            // transpose of the texture-unit sampler at the reference's FP32 coordinates
-            const RayRef32 r = ray_ref32(prm.g, p, v, u);
-            for (int i = s.i0; i < s.i1; i++)
-                run.template add<INTERP_TEXEMU>(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz,
-                                                corner_tex(ref32_coords(prm.g, r, i)), g);
-        }
-        run.flush(prm.gexp, prm.g.nx, prm.g.ny, prm.g.nz, g);
+        // the transposed weights of the forward's sampler (for the texture
+        // modes, the texture unit's, at the reference's FP32 coordinates)
+        scatter_ray_axis<M, MODE == INTERP_TRILINEAR ? INTERP_TRILINEAR : INTERP_TEXEMU>(
+            prm.g, prm.gexp, p, v, u, g, axis_is_x(prm.g, p));
     }
 }
 
-// Sums the corner-expanded accumulators into the gradient volumes:
-// g[z][y][x] += cell(z, y, x).x + cell(z, y, x-1).y + cell(z, y-1, x).z +
-// cell(z, y-1, x-1).w.  One streaming pass.
+// Sums the face accumulators of both march axes into the gradient volumes
+// (face_fold).  One streaming pass.
 template <int M>
 __global__ void k_fold(const MarchParams prm)
 {
@@ -390,13 +346,8 @@ __global__ void k_fold(const MarchParams prm)
     const int64_t n = (int64_t)nx * ny * nz;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(k % nx), y = (int)((k / nx) % ny), z = (int)(k / ((int64_t)nx * ny));
-        const size_t a = exp_index(nx, ny, x, y, z), b = exp_index(nx, ny, x - 1, y, z);
-        const size_t c = exp_index(nx, ny, x, y - 1, z), d = exp_index(nx, ny, x - 1, y - 1, z);
 #pragma unroll
-        for (int m = 0; m < M; m++) {
-            const float4* e = prm.gexp[m];
-            prm.gvol[m][k] += (e[a].x + e[b].y) + (e[c].z + e[d].w);
-        }
+        for (int m = 0; m < M; m++) prm.gvol[m][k] += face_fold(prm.gexp[m], nx, ny, nz, x, y, z);
     }
 }
 
@@ -1193,7 +1144,7 @@ cudaError_t launch_backward(const MarchParams& prm_in, int M, int interp, bool f
     return cudaSuccess;
 }
 
-size_t expanded_elems(const GeomParams& g) { return (size_t)(g.nz + 2) * (size_t)(g.ny + 1) * (size_t)(g.nx + 1); }
+size_t expanded_elems(const GeomParams& g) { return face_elems(g.nx, g.ny, g.nz); }
 
 cudaError_t launch_fold(const MarchParams& prm, int M, cudaStream_t st)
 {

@@ -22,7 +22,7 @@ struct MarchParams {
     const float* gI;                  // [P][V][U] dLoss/dI (adjoint)
     const float* gIAbs;               // [P][V][U] dLoss/dIAbsorb (adjoint, may be null)
     float* gvol[kMaxM];               // gradient volumes (adjoint)
-    float4* gexp[kMaxM];              // corner-expanded gradient accumulators (adjoint), see k_fold
+    float4* gexp[kMaxM];              // face-expanded gradient accumulators (adjoint), see AxisScatter
     int E;
     int view0;                        // first view of this launch
     int n_views;                      // views in this launch
@@ -59,12 +59,12 @@ struct LaunchShape {
 cudaError_t launch_forward(const MarchParams& prm, int M, int interp, int sampler, bool do_spectral,
                            const LaunchShape& ls, cudaStream_t st);
 cudaError_t launch_spectral_from_L(const MarchParams& prm, int M, cudaStream_t st);
-// Adjoint scatter into the corner-expanded accumulators prm.gexp (zeroed by
+// Adjoint scatter into the face-expanded accumulators prm.gexp (zeroed by
 // the caller), followed by launch_fold into prm.gvol.
 cudaError_t launch_backward(const MarchParams& prm, int M, int interp, bool from_gL, const LaunchShape& ls,
                             cudaStream_t st);
 cudaError_t launch_fold(const MarchParams& prm, int M, cudaStream_t st);
-// Elements of one corner-expanded accumulator: (nz + 2) x (ny + 1) x (nx + 1) float4.
+// Elements (float4) of one material's face-expanded accumulator (face_elems).
 size_t expanded_elems(const GeomParams& g);
 cudaError_t launch_weights(const float* spectrum, const float* grid, int grid_layout, const float* det,
                            float I0Val, int E, int U, int V, float* W, float* I0, cudaStream_t st);
