@@ -51,8 +51,23 @@ namespace {
 
 // rays of one unit (one CTA): u x v.  8 x 8 measured 3 % faster than 16 x 8
 // for the fused adjoint (more CTAs in flight per SM) and equal for the forward.
-constexpr int kTU = 8, kTV = 8;
-constexpr int kWarps = 2, kThreads = 32 * kWarps;
+// Threads of a persistent CTA, rays and views of a work unit, per kind of
+// call.  Forward: 128 threads, units of two views of a 128-ray tile (8 x 16
+// by default), the plain forward kernel's shape: 64-thread, one-view units
+// ran a single large problem 14-22 % slower than the plain kernel, the two
+// barriers and the counter atomic of every unit amortised over a quarter of
+// the rays.  Fused forward + adjoint: 64 threads, one view of a 64-ray tile
+// (8 x 8), measured 3 % faster than 128-thread units there (more CTAs in
+// flight per SM for the scatter).
+template <bool ADJOINT>
+struct BatchShape {
+    static constexpr int threads = ADJOINT ? 64 : 128;
+    static constexpr int warps = threads / 32;
+    static constexpr int vpu = ADJOINT ? 1 : 2;  // views per unit
+};
+constexpr int kTU = 8, kTV = 8;  // the fused kernel's default tile; the forward's is 8 x 16
+inline int kind_threads(int kind) { return kind ? BatchShape<true>::threads : BatchShape<false>::threads; }
+inline int kind_vpu(int kind) { return kind ? BatchShape<true>::vpu : BatchShape<false>::vpu; }
 
 // One item as the persistent kernels see it.  The pointer fields are refreshed
 // per call.
@@ -84,7 +99,7 @@ struct GroupArgs {
     int first, count;
     long long begin, end;
     unsigned long long* counter;
-    int tu_shift;  // rays of a unit (one view): (1 << tu_shift) x (kThreads >> tu_shift)
+    int tu_shift;  // rays of a unit tile: (1 << tu_shift) x (threads >> tu_shift)
 };
 
 __device__ __forceinline__ int find_item(const GroupArgs& a, long long unit)
@@ -198,43 +213,54 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     return res * res;
 }
 
-// CTAs of 64 threads per SM the kernels are compiled for (their register
-// caps: 65536 / (64 * minb)); the fused adjoint carries the scatter's run
+// CTAs per SM the kernels are compiled for (their register caps: 65536 /
+// (threads * minb): 64-thread CTAs for the fused kernels, 128-thread CTAs for
+// the forward, at the same caps as 64-thread CTAs at twice minb had); the
+// fused adjoint carries the scatter's run
 // accumulators on top of the march, and the texture emulation's FP32
 // reference coordinates take more registers than the FP64 trilinear ones.
 // For the trilinear fused adjoint, 12 CTAs (M <= 2) measured as fast as 14
-// or 16 and 2 % faster than 10 on a 12-problem batch; 8 was slower.  Every
-// cap leaves its kernel without spills (ptxas -v).
-template <bool ADJOINT, int M, int MODE>
+// or 16 and 2 % faster than 10 on a 12-problem batch; 8 was slower.  For the
+// axis sampler's 3-material forward, 12 CTAs (80 registers, spills) ran a
+// 12-problem batch 2 % slower than 10 (96 registers, none).
+template <bool ADJOINT, int M, int MODE, bool AXIS>
 struct BatchBudget {
     static constexpr int minb = MODE == INTERP_TRILINEAR
-                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : (M <= 2 ? 16 : 10))
-                                    : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 12 : 10));
+                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : (M <= 2 ? 8 : 5))
+                                    : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 6 : 5));
 };
 
 template <int M, int MODE, bool ADJOINT, bool AXIS>
-__global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb) k_batch(const GroupArgs a)
+__global__ void __launch_bounds__(BatchShape<ADJOINT>::threads, BatchBudget<ADJOINT, M, MODE, AXIS>::minb)
+    k_batch(const GroupArgs a)
 {
+    constexpr int kThreads = BatchShape<ADJOINT>::threads, kWarps = BatchShape<ADJOINT>::warps;
+    constexpr int kVPU = BatchShape<ADJOINT>::vpu;
     __shared__ float s_mu[CTFP_MAX_ENERGIES * M];
     __shared__ long long s_unit;
     __shared__ float s_loss[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the current item and its unit range: the units a CTA takes mostly fall
+    // in one item, so the item search runs only when the item changes
     int cached = -1;
+    long long c_begin = 0, c_end = 0;
     for (;;) {
         __syncthreads();  // the previous unit is done with s_mu, s_loss, s_unit
         if (threadIdx.x == 0) s_unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
         __syncthreads();
         const long long unit = s_unit;
         if (unit >= a.end) break;
-        const int k = find_item(a, unit);
+        const int k = (unit >= c_begin && unit < c_end) ? cached : find_item(a, unit);
         const ItemDesc& it = a.items[k];
         if (k != cached) {
             for (int j = threadIdx.x; j < it.E * M; j += kThreads) s_mu[j] = it.mu[j];
             cached = k;
+            c_begin = it.unit0;
+            c_end = it.unit0 + it.units;
             __syncthreads();
         }
-        // unit order within an item.  Forward: view, then tile row, then tile
-        // column.  Adjoint: tile row, then view, then tile column, so that the
+        // unit order within an item.  Forward: view pair, then tile row, then
+        // tile column.  Adjoint: tile row, then view, then tile column, so that the
         // CTAs resident at any time work on one band of detector rows over
         // many views: those rays cross a thin z-slab of the volume, whose
         // accumulator cells then stay in L2.
@@ -255,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb)
         }
         int u, v;
         const int tile_u = 1 << a.tu_shift, tile_v = kThreads >> a.tu_shift;
-        if (AXIS && tile_v % 4 == 0 && tile_u <= 16) {
+        if (AXIS && tile_v % 4 == 0 && tile_u <= kThreads / 4) {
             // the axis sampler's lane quads run down 4 detector rows
             const int q = threadIdx.x >> 2;
             u = tu * tile_u + q % tile_u;
@@ -265,7 +291,13 @@ __global__ void __launch_bounds__(kThreads, BatchBudget<ADJOINT, M, MODE>::minb)
             v = tv * tile_v + (threadIdx.x >> a.tu_shift);
         }
         float loss = 0.f;
-        if (u < it.g.U && v < it.g.V) loss = process_ray<M, MODE, ADJOINT, AXIS>(it, s_mu, p, v, u);
+        if (u < it.g.U && v < it.g.V) {
+#pragma unroll 1
+            for (int k = 0; k < kVPU; k++) {
+                const int pk = p * kVPU + k;
+                if (pk < it.g.P) loss += process_ray<M, MODE, ADJOINT, AXIS>(it, s_mu, pk, v, u);
+            }
+        }
         if (ADJOINT && it.loss) {
             for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
             if (lane == 0) s_loss[warp] = loss;
@@ -328,7 +360,7 @@ struct ctfp_batch {
     int device = 0;
     // rays of a work unit, per kind of call (0: forward, 1: forward + adjoint),
     // set by ctfp_batch_set_shape (both) or tuned per kind by ctfp_batch_autotune
-    int tile_u[2] = {kTU, kTU}, tile_v[2] = {kTV, kTV};
+    int tile_u[2] = {kTU, kTU}, tile_v[2] = {2 * kTV, kTV};
     int laid_out = -1;  // the kind the units are currently laid out for
     std::vector<ctfp_plan*> plans;
     std::vector<int> order;            // item slot -> plan index (grouped, cost order within a group)
@@ -402,7 +434,7 @@ ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>&
         GroupArgs a{table, G.first, G.count, G.begin, end, b->d_counter + gi,
                     __builtin_ctz((unsigned)b->tile_u[adjoint ? 1 : 0])};
         KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp, G.axis) : kernel_for<false>(G.M, G.interp, G.axis);
-        fn<<<G.grid[adjoint ? 1 : 0], kThreads, 0, st>>>(a);
+        fn<<<G.grid[adjoint ? 1 : 0], kind_threads(adjoint ? 1 : 0), 0, st>>>(a);
         BATCH_CUDA(cudaGetLastError());
     }
     if (adjoint && tune_div == 0) {
@@ -491,7 +523,7 @@ void layout_units(ctfp_batch* b, int kind)
         if (s == b->groups[gi].first) b->groups[gi].begin = unit;
         it.unit0 = unit;
         it.units = (long long)((g.U + b->tile_u[kind] - 1) / b->tile_u[kind]) *
-                   ((g.V + b->tile_v[kind] - 1) / b->tile_v[kind]) * g.P;
+                   ((g.V + b->tile_v[kind] - 1) / b->tile_v[kind]) * ((g.P + kind_vpu(kind) - 1) / kind_vpu(kind));
         unit += it.units;
         b->groups[gi].end = unit;
     }
@@ -624,7 +656,7 @@ ctfp_status ctfp_batch_create(int32_t n_items, ctfp_plan* const* plans, ctfp_bat
         for (int k = 0; k < 2 && e == cudaSuccess; k++) {
             int per = 0;
             KernelFn fn = k ? kernel_for<true>(G.M, G.interp, G.axis) : kernel_for<false>(G.M, G.interp, G.axis);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kThreads, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kind_threads(k), 0);
             G.grid[k] = std::max(1, per) * std::max(1, nsm);
         }
     }
@@ -709,7 +741,7 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* b, const float* const* const*
 ctfp_status ctfp_batch_set_shape(ctfp_batch* b, int32_t tile_u, int32_t tile_v)
 {
     if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
-    if (tile_u < 1 || tile_v < 1 || tile_u * tile_v != kThreads || (tile_u & (tile_u - 1)) != 0)
+    if (tile_u < 1 || tile_v < 1 || tile_u * tile_v != BatchShape<true>::threads || (tile_u & (tile_u - 1)) != 0)
         return bfail(CTFP_INVALID_ARG, "tile_u x tile_v must be 64 rays, tile_u a power of two");
     DevScope ds(b->device);
     // graphs recorded with the old queue may still be running
@@ -719,7 +751,8 @@ ctfp_status ctfp_batch_set_shape(ctfp_batch* b, int32_t tile_u, int32_t tile_v)
         G.exec = nullptr;
     }
     b->tile_u[0] = b->tile_u[1] = tile_u;
-    b->tile_v[0] = b->tile_v[1] = tile_v;
+    b->tile_v[0] = 2 * tile_v;  // the forward's 128-ray tile: the same tile, twice as high
+    b->tile_v[1] = tile_v;
     layout_units(b, 0);
     return CTFP_OK;
 }
@@ -762,6 +795,7 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     freer.a = e0;
     BATCH_CUDA(cudaEventCreate(&e1));
     freer.c = e1;
+    // 64-ray tiles; the forward's candidates are the same tiles twice as high
     static const int shapes[][2] = {{8, 8}, {16, 4}, {4, 16}, {32, 2}, {2, 32}};
     const int nshapes = (int)(sizeof(shapes) / sizeof(shapes[0]));
     int best[2] = {-1, -1};
@@ -771,7 +805,7 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     for (int kind = 0; kind < 2; kind++) {
         for (int c = 0; c < nshapes; c++) {
             b->tile_u[kind] = shapes[c][0];
-            b->tile_v[kind] = shapes[c][1];
+            b->tile_v[kind] = shapes[c][1] * (kind ? 1 : 2);
             layout_units(b, kind);
             ctfp_status rs = fill_items(b, kind);
             if (rs != CTFP_OK) return rs;
@@ -809,7 +843,7 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     }
     for (int kind = 0; kind < 2; kind++) {
         b->tile_u[kind] = shapes[best[kind]][0];
-        b->tile_v[kind] = shapes[best[kind]][1];
+        b->tile_v[kind] = shapes[best[kind]][1] * (kind ? 1 : 2);
     }
     layout_units(b, 0);
     if (out) {

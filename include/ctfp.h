@@ -297,9 +297,10 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * No counterpart in the reference, which simulates one phantom per process run
  * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
  * spectral tables; one device) and runs them with persistent kernels over a
- * device work queue: a work unit is one view x one 8 x 8 detector tile (the
- * 64 rays of one CTA; see ctfp_batch_set_shape and ctfp_batch_autotune for
- * other shapes); items are grouped by material count and sampler mode
+ * device work queue: a forward work unit is two views x one 8 x 16 detector
+ * tile (the 128 rays of one CTA), a fused forward + adjoint unit one view x
+ * one 8 x 8 tile (64 rays; see ctfp_batch_set_shape and ctfp_batch_autotune
+ * for other shapes); items are grouped by material count and sampler mode
  * (one kernel per group, each with its own register budget) and queued
  * largest first (rays x samples x materials); every CTA takes the next unit
  * from an atomic counter.  A call is recorded once as a CUDA graph (volume
@@ -336,16 +337,17 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* co
                                        float* const* const* g_volumes, float* loss, void* stream);
 
 /* Work units in the queue, persistent grid sizes of the two kernels. */
-/* Ray tile of a work unit (one view): tile_u x tile_v rays, whose product must
- * be 64, the threads of a persistent CTA, with tile_u a power of two (default
- * 8 x 8), for both kinds of call.  Waits for the device; the next call
- * re-records its graph.  (A unit holds one view: a runtime loop over several
- * views cost the persistent kernels spills.) */
+/* Ray tile of a fused forward + adjoint work unit (one view): tile_u x tile_v
+ * rays, whose product must be 64, the threads of its persistent CTA, with
+ * tile_u a power of two (default 8 x 8); the forward's units get the same
+ * tile twice as high (tile_u x 2 tile_v, 128 threads, two views).  Waits for
+ * the device; the next call re-records its graph. */
 ctfp_status ctfp_batch_set_shape(ctfp_batch* batch, int32_t tile_u, int32_t tile_v);
 /* Times, for each kind of call on its own, the forward and the fused forward
  * + loss + adjoint kernels with candidate ray tiles (8 x 8, 16 x 4, 4 x 16,
  * 32 x 2, 2 x 32) on the first eighth of every group's work queue (its
- * largest problems) and keeps the fastest tile of each kind.  Reads volumes
+ * largest problems; the forward's tiles twice as high) and keeps the fastest
+ * tile of each kind.  Reads volumes
  * and I_target as ctfp_batch_forward_adjoint does and writes nothing the
  * caller owns; out (may be NULL) receives the fused kernel's tile_u, tile_v,
  * views_per_cta = 1 and ms (ctfp_batch_get_shapes returns both tiles).

@@ -46,7 +46,10 @@ def test_batch_forward_equals_plain_calls(cuda_ok):
     items = make_items(ITEMS)
     b = Batch([it[0] for it in items])
     info = b.info()
-    assert info["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 7) // 8) * sp["views"] for sp in ITEMS)
+    # forward units: two views of an 8 x 16 ray tile (the fused kernel's 8 x 8, twice as high)
+    assert b.shapes() == {"fwd": (8, 16), "fwd_adjoint": (8, 8)}
+    assert info["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 15) // 16) * ((sp["views"] + 1) // 2)
+                                for sp in ITEMS)
     assert info["grid_forward"] % 148 == 0 and info["grid_adjoint"] % 148 == 0
     outs = b.forward([it[1] for it in items], want_L=True)
     torch.cuda.synchronize()
@@ -161,7 +164,9 @@ def test_batch_unit_shapes_equal_plain_calls(cuda_ok, shape):
     b = Batch([it[0] for it in items])
     b.set_shape(*shape)
     tu, tv = shape
-    assert b.info()["units"] == sum(((sp["U"] + tu - 1) // tu) * ((sp["V"] + tv - 1) // tv) * sp["views"]
+    tvf = 2 * tv  # the forward's tile: twice as high, two views per unit
+    assert b.shapes() == {"fwd": (tu, tvf), "fwd_adjoint": (tu, tv)}
+    assert b.info()["units"] == sum(((sp["U"] + tu - 1) // tu) * ((sp["V"] + tvf - 1) // tvf) * ((sp["views"] + 1) // 2)
                                     for sp in ITEMS)
     with pytest.raises(CtfpError):
         b.set_shape(8, 4)
@@ -192,7 +197,7 @@ def test_batch_autotune_keeps_results(cuda_ok):
     assert shape["tile_u"] * shape["tile_v"] == 64 and shape["ms"] > 0
     sh = b.shapes()  # the forward's and the fused kernel's tiles, tuned apart
     assert sh["fwd_adjoint"] == (shape["tile_u"], shape["tile_v"])
-    assert sh["fwd"][0] * sh["fwd"][1] == 64 and sh["fwd"] == (shape["fwd_tile_u"], shape["fwd_tile_v"])
+    assert sh["fwd"][0] * sh["fwd"][1] == 128 and sh["fwd"] == (shape["fwd_tile_u"], shape["fwd_tile_v"])
     assert all(float(g.abs().max()) == 0.0 for gk in grads for g in gk)
     res = b.forward_adjoint([it[1] for it in items], targets, grads=grads)
     torch.cuda.synchronize()
