@@ -158,6 +158,25 @@ def max_over_ranks(x: float, ws: int) -> float:
     return float(t.item())
 
 
+def step_times(fn, n: int, ws: int, stream) -> tuple:
+    """n back-to-back calls of fn on stream, an event recorded after each: the
+    mean ms per call over the whole run and the per-call spread (min, median,
+    max), each the max over ranks."""
+    import torch
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(n + 1)]
+    barrier_sync(ws)
+    ev[0].record(stream)
+    for k in range(n):
+        fn()
+        ev[k + 1].record(stream)
+    barrier_sync(ws)
+    per = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(n))
+    mean = max_over_ranks(ev[0].elapsed_time(ev[n]) / n, ws)
+    spread = {"min": max_over_ranks(per[0], ws), "median": max_over_ranks(per[n // 2], ws),
+              "max": max_over_ranks(per[-1], ws), "steps": n}
+    return mean, spread
+
+
 def _err_stats(x: np.ndarray) -> dict:
     return {"max": float(np.max(x)), "p99": float(np.percentile(x, 99))}
 
@@ -294,6 +313,8 @@ def main():
                     help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
                     help="problems in the uneven batch leg (0 skips it)")
+    ap.add_argument("--batch-passes", type=int, default=3,
+                    help="timed passes per arm of the batch leg (after one warm-up pass; arms interleaved)")
     ap.add_argument("--launch-shape", default=None,
                     help="tile_u,tile_v,views_per_cta,min_ctas_per_sm for the march (instead of the autotuner)")
     ap.add_argument("--no-configs", action="store_true",
@@ -494,16 +515,9 @@ def main():
 
         for _ in range(2):
             fa_step()
-        barrier_sync(ws)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n_fa = max(1, min(args.steps, 3))
-        e0.record(stream)
-        for _ in range(n_fa):
-            fa_step()
-        e1.record(stream)
-        barrier_sync(ws)
-        fa_ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
-        fa = {"value": total_rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms,
+        n_fa = max(1, min(args.steps, 10))
+        fa_ms, fa_spread = step_times(fa_step, n_fa, ws, stream)
+        fa = {"value": total_rays / (fa_ms / 1e3), "unit": "rays/s", "ms_per_step": fa_ms, "step_ms": fa_spread,
               "loss": "sum (log I - log T)^2, T = projection of the phantom x 0.97", "last_loss": float(loss)}
         fa["fused"] = None if sharded else fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays,
                                                              fa_ms, ws, stream)
@@ -728,14 +742,7 @@ def fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays, fa_ms
 
     for _ in range(2):
         step()
-    barrier_sync(ws)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(n_fa):
-        step()
-    e1.record(stream)
-    barrier_sync(ws)
-    ms = max_over_ranks(e0.elapsed_time(e1) / n_fa, ws)
+    ms, spread = step_times(step, n_fa, ws, stream)
     for x in g_f + grads:
         x.zero_()
     step()
@@ -745,7 +752,8 @@ def fused_fwd_adjoint(pr, vols, T, fa_step, grads, loss, n_fa, total_rays, fa_ms
                 for a, c in zip(g_f, grads))
     ldiff = abs(float(loss_f[0]) - float(loss)) / max(abs(float(loss)), 1e-30)
     b1.close()
-    return {"value": total_rays / (ms / 1e3), "unit": "rays/s", "ms_per_step": ms, "speedup_vs_unfused": fa_ms / ms,
+    return {"value": total_rays / (ms / 1e3), "unit": "rays/s", "ms_per_step": ms, "step_ms": spread,
+            "speedup_vs_unfused": fa_ms / ms,
             "max_rel_diff_grad_vs_unfused": gdiff, "rel_diff_loss_vs_unfused": ldiff,
             "note": "ctfp_batch_forward_adjoint on a one-item batch: forward, loss and adjoint in one "
                     "persistent kernel replayed as a CUDA graph, then the fold"}
@@ -807,8 +815,7 @@ def batch_leg(args, ws, rank, local, stream):
     def batched_fwd_adj():
         b.forward_adjoint(vols, targets, grads=grads_b, I_out=b_I, loss=loss_b)
 
-    def timed(fn):
-        fn()  # warm-up (records the batch's graph)
+    def one_pass(fn):
         barrier_sync(ws)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -817,15 +824,35 @@ def batch_leg(args, ws, rank, local, stream):
         barrier_sync(ws)
         return max_over_ranks(e0.elapsed_time(e1), ws)
 
-    t_loop_f = timed(loop_fwd)
-    t_b_f = timed(batched_fwd)
+    def timed_pair(loop_fn, batch_fn):
+        # one warm-up pass each (records the batch's graph), then the timed
+        # passes with the arms interleaved; per arm the median pass and the
+        # spread
+        loop_fn()
+        batch_fn()
+        tl, tb = [], []
+        for _ in range(max(1, args.batch_passes)):
+            tl.append(one_pass(loop_fn))
+            tb.append(one_pass(batch_fn))
+        tl.sort()
+        tb.sort()
+        return tl, tb
+
+    def arm(t_loop, t_b):
+        ml, mb = t_loop[len(t_loop) // 2], t_b[len(t_b) // 2]
+        return {"loop_rays_s": n_rays / (ml / 1e3), "batched_rays_s": n_rays / (mb / 1e3),
+                "loop_ms": ml, "batched_ms": mb, "speedup": ml / mb,
+                "loop_ms_min_max": [t_loop[0], t_loop[-1]], "batched_ms_min_max": [t_b[0], t_b[-1]],
+                "speedup_min_max": [t_loop[0] / t_b[-1], t_loop[-1] / t_b[0]], "passes": len(t_loop)}
+
+    n_rays = ws * rays
+    t_loop_f, t_b_f = timed_pair(loop_fwd, batched_fwd)
     for g in grads_loop + grads_b:
         for x in g:
             x.zero_()
-    t_loop_fa = timed(loop_fwd_adj)
-    t_b_fa = timed(batched_fwd_adj)
+    t_loop_fa, t_b_fa = timed_pair(loop_fwd_adj, batched_fwd_adj)
     torch.cuda.synchronize()
-    # both arms ran twice: gradients hold two passes each
+    # both arms ran the same number of passes into their gradients
     gerr = max(float(torch.max(torch.abs(a - c)) / torch.max(torch.abs(c)).clamp_min(1e-30))
                for ga, gc in zip(grads_b, grads_loop) for a, c in zip(ga, gc))
     ierr = max(float(torch.max(torch.abs(a["I"] - c["I"]) / c["I"].abs().clamp_min(1e-30)))
@@ -848,19 +875,18 @@ def batch_leg(args, ws, rank, local, stream):
     b.close()
     for pr in prs:
         pr.close()
-    n_rays = ws * rays
     return {
         "items": len(wl), "rays_per_pass": rays, "work_units": info["units"],
         "persistent_grid": [info["grid_forward"], info["grid_adjoint"]],
         "unit_tile": {"fwd": [unit_shape["fwd_tile_u"], unit_shape["fwd_tile_v"]],
                       "fwd_adjoint": [unit_shape["tile_u"], unit_shape["tile_v"]]},
-        "fwd": {"loop_rays_s": n_rays / (t_loop_f / 1e3), "batched_rays_s": n_rays / (t_b_f / 1e3),
-                "loop_ms": t_loop_f, "batched_ms": t_b_f, "speedup": t_loop_f / t_b_f},
-        "fwd_adjoint": {"loop_rays_s": n_rays / (t_loop_fa / 1e3), "batched_rays_s": n_rays / (t_b_fa / 1e3),
-                        "loop_ms": t_loop_fa, "batched_ms": t_b_fa, "speedup": t_loop_fa / t_b_fa},
+        "unit_views": {"fwd": unit_shape["fwd_views"], "fwd_adjoint": unit_shape["views"]},
+        "fwd": arm(t_loop_f, t_b_f),
+        "fwd_adjoint": arm(t_loop_fa, t_b_fa),
         "max_rel_diff_I_batched_vs_loop": ierr, "max_rel_diff_grad_batched_vs_loop": gerr,
         "max_rel_err_batched_I_vs_fp64_oracle": oerr,
-        "note": "one warm-up + one timed pass per arm; loop = ctfp_forward + torch dLoss/dI + ctfp_backward per problem",
+        "note": "one warm-up pass per arm, then the timed passes with the arms interleaved; ms and speedup "
+                "from the median pass; loop = ctfp_forward + torch dLoss/dI + ctfp_backward per problem",
     }
 
 

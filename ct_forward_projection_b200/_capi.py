@@ -104,6 +104,8 @@ _SIGNATURES = {
     "ctfp_batch_autotune": (C.c_int, [_P, _P, _P, _P, _P]),
     "ctfp_batch_get_shapes": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_int32)]),
+    "ctfp_batch_set_views": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "ctfp_batch_get_views": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ctfp_last_error_string": (C.c_char_p, []),
     "ctfp_version": (C.c_char_p, []),
 }

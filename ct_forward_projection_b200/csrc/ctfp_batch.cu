@@ -49,25 +49,23 @@ using namespace ctfp;
 
 namespace {
 
-// rays of one unit (one CTA): u x v.  8 x 8 measured 3 % faster than 16 x 8
-// for the fused adjoint (more CTAs in flight per SM) and equal for the forward.
-// Threads of a persistent CTA, rays and views of a work unit, per kind of
-// call.  Forward: 128 threads, units of two views of a 128-ray tile (8 x 16
-// by default), the plain forward kernel's shape: 64-thread, one-view units
-// ran a single large problem 14-22 % slower than the plain kernel, the two
-// barriers and the counter atomic of every unit amortised over a quarter of
-// the rays.  Fused forward + adjoint: 64 threads, one view of a 64-ray tile
-// (8 x 8), measured 3 % faster than 128-thread units there (more CTAs in
-// flight per SM for the scatter).
+// Threads of a persistent CTA, per kind of call, and the default rays and
+// views of a work unit.  Forward: 128 threads, units of one view of a 128-ray
+// tile (8 x 16 by default), the plain forward kernel's CTA: with the item's
+// texture handles warp-uniform (item_tex) a one-item batch runs the 36-view
+// poly_grid_256 case in 5.79 ms against 5.81 for the plain kernel, and 5.90
+// and 6.22 ms with units of 2 and 4 views.  Fused forward + adjoint: 64
+// threads, one view of a 64-ray tile (8 x 8), measured 3 % faster than
+// 128-thread units (more CTAs in flight per SM for the scatter).
 template <bool ADJOINT>
 struct BatchShape {
     static constexpr int threads = ADJOINT ? 64 : 128;
     static constexpr int warps = threads / 32;
-    static constexpr int vpu = ADJOINT ? 1 : 2;  // views per unit
 };
 constexpr int kTU = 8, kTV = 8;  // the fused kernel's default tile; the forward's is 8 x 16
+constexpr int kVPU[2] = {1, 1};  // default views per unit: forward, fused forward + adjoint
+constexpr int kMaxVPU = 8;
 inline int kind_threads(int kind) { return kind ? BatchShape<true>::threads : BatchShape<false>::threads; }
-inline int kind_vpu(int kind) { return kind ? BatchShape<true>::vpu : BatchShape<false>::vpu; }
 
 // One item as the persistent kernels see it.  The pointer fields are refreshed
 // per call.
@@ -81,6 +79,7 @@ struct ItemDesc {
     const float* W;    // [E][V][U]
     int M, E, interp;
     int tiles_u, tiles_v;
+    int vgroups;       // groups of views per unit: ceil(P / views per unit)
     long long unit0;   // first unit of this item in the batch's numbering
     long long units;
     // per call
@@ -100,6 +99,7 @@ struct GroupArgs {
     long long begin, end;
     unsigned long long* counter;
     int tu_shift;  // rays of a unit tile: (1 << tu_shift) x (threads >> tu_shift)
+    int vpu;       // views per unit
 };
 
 __device__ __forceinline__ int find_item(const GroupArgs& a, long long unit)
@@ -111,6 +111,41 @@ __device__ __forceinline__ int find_item(const GroupArgs& a, long long unit)
         else hi = mid - 1;
     }
     return lo;
+}
+
+// The texture handles of the current item, read once per work unit through
+// warp reductions of their two halves.  Every lane of a CTA holds the same
+// item, but a value loaded from the item table is not known to be warp-uniform
+// to the compiler, which must then assume a different texture per lane at
+// every gather; the reductions' results are uniform by construction.  (All 32
+// lanes of the warp execute this.)
+template <int M>
+struct ItemTex {
+    cudaTextureObject_t x[M], y[M], l[M], t[M];
+};
+__device__ __forceinline__ cudaTextureObject_t warp_uniform(cudaTextureObject_t h)
+{
+    const unsigned lo = __reduce_min_sync(0xffffffffu, (unsigned)h);
+    const unsigned hi = __reduce_min_sync(0xffffffffu, (unsigned)(h >> 32));
+    return ((cudaTextureObject_t)hi << 32) | lo;
+}
+template <int M, int MODE, bool AXIS>
+__device__ __forceinline__ ItemTex<M> item_tex(const ItemDesc& it)
+{
+    ItemTex<M> r;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        r.x[m] = r.y[m] = r.l[m] = r.t[m] = 0;
+        if (MODE == INTERP_TEXTURE) {
+            r.t[m] = warp_uniform(it.tex[m]);
+        } else if (AXIS) {
+            r.x[m] = warp_uniform(it.xtex[m]);
+            r.y[m] = warp_uniform(it.ytex[m]);
+        } else {
+            r.l[m] = warp_uniform(it.ltex[m]);
+        }
+    }
+    return r;
 }
 
 template <int MODE>
@@ -127,14 +162,14 @@ __device__ __forceinline__ Corner batch_corner(const ItemDesc& it, const RaySeg&
 // in TEXTURE mode the hardware tex3D at the reference's FP32 coordinates (as
 // k_forward).
 template <int M, int MODE, bool AXIS>
-__device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s, const RayRef32& r, int p, int v,
-                                            int u, float* L)
+__device__ __forceinline__ void batch_march(const ItemDesc& it, const ItemTex<M>& tx, const RaySeg& s,
+                                            const RayRef32& r, int p, int v, int u, float* L)
 {
     if (AXIS && MODE != INTERP_TEXTURE) {
         const OccView none{nullptr, 0, 0, 0, 0, 0, 0};
         constexpr int AM = MODE == INTERP_TEXTURE ? INTERP_TEXEMU : MODE;  // (not instantiated for TEXTURE)
-        if (axis_is_x(it.g, p)) march_ray_axis<M, AM, 0, false>(it.g, it.xtex, it.ytex, none, p, v, u, L);
-        else march_ray_axis<M, AM, 1, false>(it.g, it.xtex, it.ytex, none, p, v, u, L);
+        if (axis_is_x(it.g, p)) march_ray_axis<M, AM, 0, false>(it.g, tx.x, tx.y, none, p, v, u, L);
+        else march_ray_axis<M, AM, 1, false>(it.g, tx.x, tx.y, none, p, v, u, L);
         return;
     }
     float acc[M], cmp[M];
@@ -145,7 +180,7 @@ __device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s,
         for (int i = s.i0; i < s.i1; i++) {
             const float3 x = ref32_coords(it.g, r, i);
 #pragma unroll
-            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(it.tex[m], x.x, x.y, x.z));
+            for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(tx.t[m], x.x, x.y, x.z));
         }
 #pragma unroll
         for (int m = 0; m < M; m++) L[m] = it.g.dx * (acc[m] - cmp[m]);
@@ -155,7 +190,7 @@ __device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s,
     for (int i = s.i0; i < s.i1; i++) {
         const Corner c = batch_corner<MODE>(it, s, r, i);
         float v[M][8];
-        load8_layered<M>(it.ltex, it.g.nz, c, v);
+        load8_layered<M>(tx.l, it.g.nz, c, v);
 #pragma unroll
         for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], interp8<MODE>(c, v[m]));
     }
@@ -168,7 +203,8 @@ __device__ __forceinline__ void batch_march(const ItemDesc& it, const RaySeg& s,
 // One ray.  ADJOINT: the fused forward + loss + adjoint; returns the ray's
 // loss term.
 template <int M, int MODE, bool ADJOINT, bool AXIS>
-__device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_mu, int p, int v, int u)
+__device__ __forceinline__ float process_ray(const ItemDesc& it, const ItemTex<M>& tx, const float* s_mu, int p, int v,
+                                             int u)
 {
     const int64_t npix = (int64_t)it.g.U * it.g.V;
     const int64_t pix = (int64_t)v * it.g.U + u;
@@ -177,7 +213,7 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const float* s_
     RayRef32 r;
     if (MODE != INTERP_TRILINEAR) r = ray_ref32(it.g, p, v, u);
     float L[M];
-    batch_march<M, MODE, AXIS>(it, s, r, p, v, u, L);
+    batch_march<M, MODE, AXIS>(it, tx, s, r, p, v, u, L);
     // the plain forward's epilogue (spectral / spectral_adjoint), so the
     // batch's I equals ctfp_forward's for the same path integrals
     if (!ADJOINT) {
@@ -230,12 +266,14 @@ struct BatchBudget {
                                     : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 6 : 5));
 };
 
-template <int M, int MODE, bool ADJOINT, bool AXIS>
+// MULTI: units of more than one view (a.vpu > 1), marched one view after the
+// other; the one-view kernel has no view loop, whose live state cost the fused
+// axis kernel 3 % on the 48-problem batch.
+template <int M, int MODE, bool ADJOINT, bool AXIS, bool MULTI>
 __global__ void __launch_bounds__(BatchShape<ADJOINT>::threads, BatchBudget<ADJOINT, M, MODE, AXIS>::minb)
     k_batch(const GroupArgs a)
 {
     constexpr int kThreads = BatchShape<ADJOINT>::threads, kWarps = BatchShape<ADJOINT>::warps;
-    constexpr int kVPU = BatchShape<ADJOINT>::vpu;
     __shared__ float s_mu[CTFP_MAX_ENERGIES * M];
     __shared__ long long s_unit;
     __shared__ float s_loss[kWarps];
@@ -259,15 +297,16 @@ __global__ void __launch_bounds__(BatchShape<ADJOINT>::threads, BatchBudget<ADJO
             c_end = it.unit0 + it.units;
             __syncthreads();
         }
-        // unit order within an item.  Forward: view pair, then tile row, then
-        // tile column.  Adjoint: tile row, then view, then tile column, so that the
-        // CTAs resident at any time work on one band of detector rows over
-        // many views: those rays cross a thin z-slab of the volume, whose
-        // accumulator cells then stay in L2.
+        const ItemTex<M> tx = item_tex<M, MODE, AXIS>(it);
+        // unit order within an item.  Forward: view group, then tile row, then
+        // tile column.  Adjoint: tile row, then view group, then tile column,
+        // so that the CTAs resident at any time work on one band of detector
+        // rows over many views: those rays cross a thin z-slab of the volume,
+        // whose accumulator cells then stay in L2.
         const long long local = unit - it.unit0;
         int p, tu, tv;
         if (ADJOINT) {
-            const long long band_units = (long long)it.g.P * it.tiles_u;
+            const long long band_units = (long long)it.vgroups * it.tiles_u;
             tv = (int)(local / band_units);
             const int rem = (int)(local % band_units);
             p = rem / it.tiles_u;
@@ -292,10 +331,13 @@ __global__ void __launch_bounds__(BatchShape<ADJOINT>::threads, BatchBudget<ADJO
         }
         float loss = 0.f;
         if (u < it.g.U && v < it.g.V) {
+            if (!MULTI) {
+                loss = process_ray<M, MODE, ADJOINT, AXIS>(it, tx, s_mu, p, v, u);
+            } else {
+                const int p_end = min((p + 1) * a.vpu, it.g.P);
 #pragma unroll 1
-            for (int k = 0; k < kVPU; k++) {
-                const int pk = p * kVPU + k;
-                if (pk < it.g.P) loss += process_ray<M, MODE, ADJOINT, AXIS>(it, s_mu, pk, v, u);
+                for (int pk = p * a.vpu; pk < p_end; pk++)
+                    loss += process_ray<M, MODE, ADJOINT, AXIS>(it, tx, s_mu, pk, v, u);
             }
         }
         if (ADJOINT && it.loss) {
@@ -332,25 +374,34 @@ __global__ void k_batch_fold(const ItemDesc* items, int n_items, const long long
 
 using KernelFn = void (*)(GroupArgs);
 
-template <int M, bool ADJOINT>
+template <int M, bool ADJOINT, bool MULTI>
 KernelFn kernel_for_m(int interp, bool axis)
 {
     if (interp == INTERP_TRILINEAR)
-        return axis ? k_batch<M, INTERP_TRILINEAR, ADJOINT, true> : k_batch<M, INTERP_TRILINEAR, ADJOINT, false>;
+        return axis ? k_batch<M, INTERP_TRILINEAR, ADJOINT, true, MULTI>
+                    : k_batch<M, INTERP_TRILINEAR, ADJOINT, false, MULTI>;
     if (interp == INTERP_TEXEMU)
-        return axis ? k_batch<M, INTERP_TEXEMU, ADJOINT, true> : k_batch<M, INTERP_TEXEMU, ADJOINT, false>;
-    return k_batch<M, INTERP_TEXTURE, ADJOINT, false>;
+        return axis ? k_batch<M, INTERP_TEXEMU, ADJOINT, true, MULTI> : k_batch<M, INTERP_TEXEMU, ADJOINT, false, MULTI>;
+    return k_batch<M, INTERP_TEXTURE, ADJOINT, false, MULTI>;
 }
 
-template <bool ADJOINT>
-KernelFn kernel_for(int M, int interp, bool axis)
+template <bool ADJOINT, bool MULTI>
+KernelFn kernel_for_v(int M, int interp, bool axis)
 {
     switch (M) {
-        case 1: return kernel_for_m<1, ADJOINT>(interp, axis);
-        case 2: return kernel_for_m<2, ADJOINT>(interp, axis);
-        case 3: return kernel_for_m<3, ADJOINT>(interp, axis);
-        default: return kernel_for_m<4, ADJOINT>(interp, axis);
+        case 1: return kernel_for_m<1, ADJOINT, MULTI>(interp, axis);
+        case 2: return kernel_for_m<2, ADJOINT, MULTI>(interp, axis);
+        case 3: return kernel_for_m<3, ADJOINT, MULTI>(interp, axis);
+        default: return kernel_for_m<4, ADJOINT, MULTI>(interp, axis);
     }
+}
+
+// The kernel of one kind of call for units of vpu views (both variants have
+// the same register budget, hence the same persistent grid).
+template <bool ADJOINT>
+KernelFn kernel_for(int M, int interp, bool axis, int vpu = 1)
+{
+    return vpu > 1 ? kernel_for_v<ADJOINT, true>(M, interp, axis) : kernel_for_v<ADJOINT, false>(M, interp, axis);
 }
 
 }  // namespace
@@ -358,9 +409,11 @@ KernelFn kernel_for(int M, int interp, bool axis)
 struct ctfp_batch {
     int n = 0;
     int device = 0;
-    // rays of a work unit, per kind of call (0: forward, 1: forward + adjoint),
-    // set by ctfp_batch_set_shape (both) or tuned per kind by ctfp_batch_autotune
+    // rays and views of a work unit, per kind of call (0: forward, 1: forward
+    // + adjoint), set by ctfp_batch_set_shape and ctfp_batch_set_views or
+    // tuned per kind by ctfp_batch_autotune
     int tile_u[2] = {kTU, kTU}, tile_v[2] = {2 * kTV, kTV};
+    int vpu[2] = {kVPU[0], kVPU[1]};
     int laid_out = -1;  // the kind the units are currently laid out for
     std::vector<ctfp_plan*> plans;
     std::vector<int> order;            // item slot -> plan index (grouped, cost order within a group)
@@ -432,8 +485,10 @@ ctfp_status record(ctfp_batch* b, bool adjoint, const std::vector<const float*>&
         // tuning runs the first 1/tune_div of each group's queue: its largest items
         const long long end = tune_div > 0 ? G.begin + std::max(1LL, (G.end - G.begin) / tune_div) : G.end;
         GroupArgs a{table, G.first, G.count, G.begin, end, b->d_counter + gi,
-                    __builtin_ctz((unsigned)b->tile_u[adjoint ? 1 : 0])};
-        KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp, G.axis) : kernel_for<false>(G.M, G.interp, G.axis);
+                    __builtin_ctz((unsigned)b->tile_u[adjoint ? 1 : 0]), b->vpu[adjoint ? 1 : 0]};
+        const int vpu = b->vpu[adjoint ? 1 : 0];
+        KernelFn fn = adjoint ? kernel_for<true>(G.M, G.interp, G.axis, vpu)
+                              : kernel_for<false>(G.M, G.interp, G.axis, vpu);
         fn<<<G.grid[adjoint ? 1 : 0], kind_threads(adjoint ? 1 : 0), 0, st>>>(a);
         BATCH_CUDA(cudaGetLastError());
     }
@@ -510,7 +565,8 @@ bool batchable(const ctfp_plan* p)
 bool uses_axis(const ctfp_plan* p) { return plan_interp(p) != INTERP_TEXTURE && plan_sampler(p) == SAMPLER_AXIS; }
 
 // Unit counts and queue ranges for the unit shape of one kind of call: item s
-// holds tiles_u x tiles_v x P units, numbered after the items before it.
+// holds tiles_u x tiles_v x ceil(P / views per unit) units, numbered after the
+// items before it.
 void layout_units(ctfp_batch* b, int kind)
 {
     b->laid_out = kind;
@@ -523,7 +579,7 @@ void layout_units(ctfp_batch* b, int kind)
         if (s == b->groups[gi].first) b->groups[gi].begin = unit;
         it.unit0 = unit;
         it.units = (long long)((g.U + b->tile_u[kind] - 1) / b->tile_u[kind]) *
-                   ((g.V + b->tile_v[kind] - 1) / b->tile_v[kind]) * ((g.P + kind_vpu(kind) - 1) / kind_vpu(kind));
+                   ((g.V + b->tile_v[kind] - 1) / b->tile_v[kind]) * ((g.P + b->vpu[kind] - 1) / b->vpu[kind]);
         unit += it.units;
         b->groups[gi].end = unit;
     }
@@ -563,6 +619,7 @@ ctfp_status fill_items(ctfp_batch* b, int kind)
         }
         it.tiles_u = (it.g.U + b->tile_u[kind] - 1) / b->tile_u[kind];
         it.tiles_v = (it.g.V + b->tile_v[kind] - 1) / b->tile_v[kind];
+        it.vgroups = (it.g.P + b->vpu[kind] - 1) / b->vpu[kind];
         it.unit0 = unit0;
         it.units = units;
     }
@@ -757,6 +814,31 @@ ctfp_status ctfp_batch_set_shape(ctfp_batch* b, int32_t tile_u, int32_t tile_v)
     return CTFP_OK;
 }
 
+ctfp_status ctfp_batch_set_views(ctfp_batch* b, int32_t fwd_views, int32_t adj_views)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (fwd_views < 1 || fwd_views > kMaxVPU || adj_views < 1 || adj_views > kMaxVPU)
+        return bfail(CTFP_INVALID_ARG, "views per work unit must be in [1, 8]");
+    DevScope ds(b->device);
+    BATCH_CUDA(cudaDeviceSynchronize());
+    for (ctfp_batch::Graph& G : b->graph) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+    }
+    b->vpu[0] = fwd_views;
+    b->vpu[1] = adj_views;
+    layout_units(b, 0);
+    return CTFP_OK;
+}
+
+ctfp_status ctfp_batch_get_views(const ctfp_batch* b, int32_t* fwd_views, int32_t* adj_views)
+{
+    if (!b) return bfail(CTFP_INVALID_ARG, "batch is NULL");
+    if (fwd_views) *fwd_views = b->vpu[0];
+    if (adj_views) *adj_views = b->vpu[1];
+    return CTFP_OK;
+}
+
 ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volumes, const float* const* I_target,
                                 ctfp_launch_shape* out, void* stream)
 {
@@ -798,39 +880,60 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     // 64-ray tiles; the forward's candidates are the same tiles twice as high
     static const int shapes[][2] = {{8, 8}, {16, 4}, {4, 16}, {32, 2}, {2, 32}};
     const int nshapes = (int)(sizeof(shapes) / sizeof(shapes[0]));
-    int best[2] = {-1, -1};
+    static const int views[] = {1, 2, 4};
+    const int nviews = (int)(sizeof(views) / sizeof(views[0]));
+    // times one candidate unit shape of one kind on its own kernel
+    auto time_shape = [&](int kind, int c, int vpu, float& ms) -> ctfp_status {
+        b->tile_u[kind] = shapes[c][0];
+        b->tile_v[kind] = shapes[c][1] * (kind ? 1 : 2);
+        b->vpu[kind] = vpu;
+        layout_units(b, kind);
+        ctfp_status rs = fill_items(b, kind);
+        if (rs != CTFP_OK) return rs;
+        for (int s = 0; s < b->n; s++) {
+            ItemDesc& it = b->items[(size_t)s];
+            it.I_target = I_target[b->order[(size_t)s]];
+            it.loss = kind ? loss + b->order[(size_t)s] : nullptr;
+            it.I = nullptr;  // the forward's outputs go nowhere while tuning
+            it.IAbs = nullptr;
+            it.L = nullptr;
+        }
+        BATCH_CUDA(cudaStreamSynchronize(st));
+        BATCH_CUDA(cudaMemcpy(b->d_items[kind], b->items.data(), sizeof(ItemDesc) * (size_t)b->n,
+                              cudaMemcpyHostToDevice));
+        rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);  // warm-up
+        if (rs != CTFP_OK) return rs;
+        BATCH_CUDA(cudaEventRecord(e0, st));
+        rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);
+        if (rs != CTFP_OK) return rs;
+        BATCH_CUDA(cudaEventRecord(e1, st));
+        BATCH_CUDA(cudaEventSynchronize(e1));
+        BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return CTFP_OK;
+    };
+    int best[2] = {-1, -1}, best_vpu[2] = {b->vpu[0], b->vpu[1]};
     float best_ms[2] = {0.f, 0.f};
-    // each kind of call on its own kernel: the forward, then the fused
-    // forward + adjoint
+    // each kind of call on its own kernel, the forward, then the fused forward
+    // + adjoint: the tiles at the kind's current views per unit, then the
+    // views per unit with the fastest tile
     for (int kind = 0; kind < 2; kind++) {
+        const int vpu0 = b->vpu[kind];
         for (int c = 0; c < nshapes; c++) {
-            b->tile_u[kind] = shapes[c][0];
-            b->tile_v[kind] = shapes[c][1] * (kind ? 1 : 2);
-            layout_units(b, kind);
-            ctfp_status rs = fill_items(b, kind);
-            if (rs != CTFP_OK) return rs;
-            for (int s = 0; s < b->n; s++) {
-                ItemDesc& it = b->items[(size_t)s];
-                it.I_target = I_target[b->order[(size_t)s]];
-                it.loss = kind ? loss + b->order[(size_t)s] : nullptr;
-                it.I = nullptr;  // the forward's outputs go nowhere while tuning
-                it.IAbs = nullptr;
-                it.L = nullptr;
-            }
-            BATCH_CUDA(cudaStreamSynchronize(st));
-            BATCH_CUDA(cudaMemcpy(b->d_items[kind], b->items.data(), sizeof(ItemDesc) * (size_t)b->n,
-                                  cudaMemcpyHostToDevice));
-            rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);  // warm-up
-            if (rs != CTFP_OK) return rs;
-            BATCH_CUDA(cudaEventRecord(e0, st));
-            rs = record(b, kind == 1, vols, kind ? loss : nullptr, st, 8);
-            if (rs != CTFP_OK) return rs;
-            BATCH_CUDA(cudaEventRecord(e1, st));
-            BATCH_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
-            BATCH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const ctfp_status rs = time_shape(kind, c, vpu0, ms);
+            if (rs != CTFP_OK) return rs;
             if (best[kind] < 0 || ms < best_ms[kind]) {
                 best[kind] = c;
+                best_ms[kind] = ms;
+            }
+        }
+        for (int j = 0; j < nviews; j++) {
+            if (views[j] == vpu0) continue;
+            float ms = 0.f;
+            const ctfp_status rs = time_shape(kind, best[kind], views[j], ms);
+            if (rs != CTFP_OK) return rs;
+            if (ms < best_ms[kind]) {
+                best_vpu[kind] = views[j];
                 best_ms[kind] = ms;
             }
         }
@@ -844,12 +947,13 @@ ctfp_status ctfp_batch_autotune(ctfp_batch* b, const float* const* const* volume
     for (int kind = 0; kind < 2; kind++) {
         b->tile_u[kind] = shapes[best[kind]][0];
         b->tile_v[kind] = shapes[best[kind]][1] * (kind ? 1 : 2);
+        b->vpu[kind] = best_vpu[kind];
     }
     layout_units(b, 0);
     if (out) {
         out->tile_u = shapes[best[1]][0];
         out->tile_v = shapes[best[1]][1];
-        out->views_per_cta = 1;
+        out->views_per_cta = best_vpu[1];
         out->min_ctas_per_sm = 0;
         out->ms = best_ms[1];
         out->from_cache = 0;

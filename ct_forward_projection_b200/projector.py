@@ -358,24 +358,35 @@ class Batch:
         """ctfp_batch_set_shape: tile_u x tile_v (= 64) rays per work unit."""
         call("ctfp_batch_set_shape", self._h, tile_u, tile_v)
 
+    def set_views(self, fwd_views: int, adj_views: int) -> None:
+        """ctfp_batch_set_views: views per work unit of the forward and of the
+        fused forward + adjoint (1 to 8)."""
+        call("ctfp_batch_set_views", self._h, fwd_views, adj_views)
+
     def autotune(self, volumes: Sequence[Sequence], targets: Sequence, stream=None) -> dict:
         """ctfp_batch_autotune: times the forward and the fused kernels with
-        candidate unit shapes and keeps the fastest of each; returns the fused
-        kernel's tile (tile_u, tile_v, ms) and the forward's (fwd_tile_u, fwd_tile_v)."""
+        candidate ray tiles and views per unit and keeps the fastest of each;
+        returns the fused kernel's tile (tile_u, tile_v), views per unit and
+        ms, and the forward's tile (fwd_tile_u, fwd_tile_v) and views."""
         self._keep = []
         vt = self._vol_table(volumes)
         T = self._item_ptrs(targets, 1, "target")
         r = capi.LaunchShape()
         call("ctfp_batch_autotune", self._h, vt, T, C.byref(r), _stream(stream))
         sh = self.shapes()
-        return {"tile_u": r.tile_u, "tile_v": r.tile_v, "ms": r.ms, "fwd_tile_u": sh["fwd"][0],
-                "fwd_tile_v": sh["fwd"][1]}
+        return {"tile_u": r.tile_u, "tile_v": r.tile_v, "views": r.views_per_cta, "ms": r.ms,
+                "fwd_tile_u": sh["fwd"][0], "fwd_tile_v": sh["fwd"][1], "fwd_views": sh["views"][0]}
 
     def shapes(self) -> dict:
-        """ctfp_batch_get_shapes: the work-unit ray tiles of the two kinds of call."""
+        """ctfp_batch_get_shapes and ctfp_batch_get_views: the work-unit ray
+        tiles of the two kinds of call, and their views per unit
+        ("views": (forward, fused))."""
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         call("ctfp_batch_get_shapes", self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
-        return {"fwd": (int(a.value), int(b.value)), "fwd_adjoint": (int(c.value), int(d.value))}
+        f, j = C.c_int32(), C.c_int32()
+        call("ctfp_batch_get_views", self._h, C.byref(f), C.byref(j))
+        return {"fwd": (int(a.value), int(b.value)), "fwd_adjoint": (int(c.value), int(d.value)),
+                "views": (int(f.value), int(j.value))}
 
     def info(self) -> dict:
         u, g0, g1 = C.c_int64(), C.c_int32(), C.c_int32()

@@ -297,10 +297,10 @@ ctfp_status ctfp_plan_autotune(ctfp_plan* plan, const float* const* volumes, flo
  * No counterpart in the reference, which simulates one phantom per process run
  * (Source/Main_Forward_Projection_V1.1.cpp:18-23).  A batch holds n_items plans (own geometry, materials,
  * spectral tables; one device) and runs them with persistent kernels over a
- * device work queue: a forward work unit is two views x one 8 x 16 detector
+ * device work queue: a forward work unit is one view x one 8 x 16 detector
  * tile (the 128 rays of one CTA), a fused forward + adjoint unit one view x
- * one 8 x 8 tile (64 rays; see ctfp_batch_set_shape and ctfp_batch_autotune
- * for other shapes); items are grouped by material count and sampler mode
+ * one 8 x 8 tile (64 rays; see ctfp_batch_set_shape, ctfp_batch_set_views
+ * and ctfp_batch_autotune for other shapes); items are grouped by material count and sampler mode
  * (one kernel per group, each with its own register budget) and queued
  * largest first (rays x samples x materials); every CTA takes the next unit
  * from an atomic counter.  A call is recorded once as a CUDA graph (volume
@@ -343,14 +343,21 @@ ctfp_status ctfp_batch_forward_adjoint(ctfp_batch* batch, const float* const* co
  * tile twice as high (tile_u x 2 tile_v, 128 threads, two views).  Waits for
  * the device; the next call re-records its graph. */
 ctfp_status ctfp_batch_set_shape(ctfp_batch* batch, int32_t tile_u, int32_t tile_v);
+/* Views of a work unit, per kind of call (1 to 8, default 1): a unit marches
+ * its rays for that many consecutive views, one after the other, so the
+ * unit's queue atomic, barriers and item lookup are spread over more rays.
+ * Waits for the device; the next call re-records its graph. */
+ctfp_status ctfp_batch_set_views(ctfp_batch* batch, int32_t fwd_views, int32_t adj_views);
+ctfp_status ctfp_batch_get_views(const ctfp_batch* batch, int32_t* fwd_views, int32_t* adj_views);
 /* Times, for each kind of call on its own, the forward and the fused forward
- * + loss + adjoint kernels with candidate ray tiles (8 x 8, 16 x 4, 4 x 16,
- * 32 x 2, 2 x 32) on the first eighth of every group's work queue (its
- * largest problems; the forward's tiles twice as high) and keeps the fastest
- * tile of each kind.  Reads volumes
- * and I_target as ctfp_batch_forward_adjoint does and writes nothing the
- * caller owns; out (may be NULL) receives the fused kernel's tile_u, tile_v,
- * views_per_cta = 1 and ms (ctfp_batch_get_shapes returns both tiles).
+ * + loss + adjoint kernels on the first eighth of every group's work queue
+ * (its largest problems): the candidate ray tiles (8 x 8, 16 x 4, 4 x 16,
+ * 32 x 2, 2 x 32; the forward's twice as high) at the kind's current views
+ * per unit, then 1, 2 and 4 views per unit with the fastest tile, and keeps
+ * the fastest tile and views of each kind.  Reads volumes and I_target as
+ * ctfp_batch_forward_adjoint does and writes nothing the caller owns; out
+ * (may be NULL) receives the fused kernel's tile_u, tile_v, views_per_cta and
+ * ms (ctfp_batch_get_shapes and ctfp_batch_get_views return both kinds').
  * Waits for the device. */
 ctfp_status ctfp_batch_autotune(ctfp_batch* batch, const float* const* const* volumes, const float* const* I_target,
                                 ctfp_launch_shape* out, void* stream);

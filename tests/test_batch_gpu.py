@@ -46,10 +46,9 @@ def test_batch_forward_equals_plain_calls(cuda_ok):
     items = make_items(ITEMS)
     b = Batch([it[0] for it in items])
     info = b.info()
-    # forward units: two views of an 8 x 16 ray tile (the fused kernel's 8 x 8, twice as high)
-    assert b.shapes() == {"fwd": (8, 16), "fwd_adjoint": (8, 8)}
-    assert info["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 15) // 16) * ((sp["views"] + 1) // 2)
-                                for sp in ITEMS)
+    # forward units: one view of an 8 x 16 ray tile (the fused kernel's 8 x 8, twice as high)
+    assert b.shapes() == {"fwd": (8, 16), "fwd_adjoint": (8, 8), "views": (1, 1)}
+    assert info["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 15) // 16) * sp["views"] for sp in ITEMS)
     assert info["grid_forward"] % 148 == 0 and info["grid_adjoint"] % 148 == 0
     outs = b.forward([it[1] for it in items], want_L=True)
     torch.cuda.synchronize()
@@ -164,9 +163,9 @@ def test_batch_unit_shapes_equal_plain_calls(cuda_ok, shape):
     b = Batch([it[0] for it in items])
     b.set_shape(*shape)
     tu, tv = shape
-    tvf = 2 * tv  # the forward's tile: twice as high, two views per unit
-    assert b.shapes() == {"fwd": (tu, tvf), "fwd_adjoint": (tu, tv)}
-    assert b.info()["units"] == sum(((sp["U"] + tu - 1) // tu) * ((sp["V"] + tvf - 1) // tvf) * ((sp["views"] + 1) // 2)
+    tvf = 2 * tv  # the forward's tile: twice as high
+    assert b.shapes() == {"fwd": (tu, tvf), "fwd_adjoint": (tu, tv), "views": (1, 1)}
+    assert b.info()["units"] == sum(((sp["U"] + tu - 1) // tu) * ((sp["V"] + tvf - 1) // tvf) * sp["views"]
                                     for sp in ITEMS)
     with pytest.raises(CtfpError):
         b.set_shape(8, 4)
@@ -176,6 +175,40 @@ def test_batch_unit_shapes_equal_plain_calls(cuda_ok, shape):
         ref = pr.forward(vols, want_L=True)
         torch.cuda.synchronize()
         assert rel(o["I"], ref["I"]) < 2e-6 and rel(o["L"], ref["L"]) < 1e-6
+    b.close()
+
+
+@pytest.mark.parametrize("views", [(1, 2), (4, 4), (3, 1)])
+def test_batch_views_per_unit(cuda_ok, views):
+    # a unit marches its rays for several consecutive views: every ray of every
+    # view still runs exactly once, forward and fused
+    items = make_items(ITEMS)
+    b = Batch([it[0] for it in items])
+    with pytest.raises(CtfpError):
+        b.set_views(0, 1)
+    with pytest.raises(CtfpError):
+        b.set_views(1, 9)
+    b.set_views(*views)
+    fv, av = views
+    assert b.shapes()["views"] == views
+    assert b.info()["units"] == sum(((sp["U"] + 7) // 8) * ((sp["V"] + 15) // 16) * ((sp["views"] + fv - 1) // fv)
+                                    for sp in ITEMS)
+    outs = b.forward([it[1] for it in items], want_L=True)
+    targets, ref_grads = [], []
+    for (pr, vols, _), o in zip(items, outs):
+        ref = pr.forward(vols, want_L=True)
+        torch.cuda.synchronize()
+        assert rel(o["I"], ref["I"]) < 2e-6 and rel(o["L"], ref["L"]) < 1e-6
+        T = (ref["I"] * 0.98).contiguous()
+        targets.append(T)
+        r = torch.log(ref["I"].double()) - torch.log(T.double())
+        ref_grads.append(pr.backward(ref["L"], gI=(2.0 * r / ref["I"].double()).float()))
+    grads = [[torch.zeros_like(v) for v in it[1]] for it in items]
+    res = b.forward_adjoint([it[1] for it in items], targets, grads=grads)
+    torch.cuda.synchronize()
+    for k, (pr, _, _) in enumerate(items):
+        for m in range(pr.M):
+            assert rel(res["grads"][k][m], ref_grads[k][m]) < 1e-4
     b.close()
 
 
@@ -195,9 +228,10 @@ def test_batch_autotune_keeps_results(cuda_ok):
     grads = [[torch.zeros_like(v) for v in it[1]] for it in items]
     shape = b.autotune([it[1] for it in items], targets)
     assert shape["tile_u"] * shape["tile_v"] == 64 and shape["ms"] > 0
-    sh = b.shapes()  # the forward's and the fused kernel's tiles, tuned apart
+    sh = b.shapes()  # the forward's and the fused kernel's tiles and views, tuned apart
     assert sh["fwd_adjoint"] == (shape["tile_u"], shape["tile_v"])
     assert sh["fwd"][0] * sh["fwd"][1] == 128 and sh["fwd"] == (shape["fwd_tile_u"], shape["fwd_tile_v"])
+    assert sh["views"] == (shape["fwd_views"], shape["views"]) and set(sh["views"]) <= {1, 2, 4}
     assert all(float(g.abs().max()) == 0.0 for gk in grads for g in gk)
     res = b.forward_adjoint([it[1] for it in items], targets, grads=grads)
     torch.cuda.synchronize()
