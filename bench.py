@@ -43,7 +43,12 @@ HBM_FALLBACK_GBS = 6650.0
 # (dram__bytes_read.sum + dram__bytes_write.sum) of k_forward on the 36-view
 # case of the same problem (poly_grid_256_v36, default launch shape): 5.95 GB +
 # 0.09 GB, scaled by 10 for 360 views (traffic grows with the views marched).
-TRAFFIC_PER_LAUNCH = {("poly_grid_256", "trilinear", "layered"): 60.37e9}
+# DRAM bytes (read + write) of one forward launch over the 360-view workload:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 36-view
+# case (every tenth view), x10.  An upper estimate: in the full run adjacent
+# views are 1 degree apart and share more L2 lines than the 36-view case's.
+TRAFFIC_PER_LAUNCH = {("poly_grid_256", "trilinear", "layered"): 60.37e9,
+                      ("poly_grid_256", "trilinear", "axis"): 73.20e9}
 BYTES_PER_VOXEL_SAMPLE = 32  # 8 FP32 corners, the reuse-free trilinear footprint
 
 
@@ -456,7 +461,8 @@ def main():
                 "traffic": traffic,
                 "traffic_source": None if traffic is None else
                     "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
-                    "the 36-view case of this workload, x10 for 360 views (the committed ncu summary of this kernel)",
+                    "the 36-view case of this workload (every tenth view), x10 for 360 views (the committed ncu "
+                    "summary of this kernel); an upper estimate, adjacent views sharing more L2 lines in the full run",
                 "voxel_samples_per_launch": vs_launch, "voxel_samples_per_s": vs_rate,
                 "nominal_voxel_samples_per_launch": nominal_vs,
                 "hbm": {"compulsory_bytes_per_launch": compulsory,

@@ -250,19 +250,20 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const ItemTex<M
 }
 
 // CTAs per SM the kernels are compiled for (their register caps: 65536 /
-// (threads * minb): 64-thread CTAs for the fused kernels, 128-thread CTAs for
-// the forward, at the same caps as 64-thread CTAs at twice minb had); the
-// fused adjoint carries the scatter's run
-// accumulators on top of the march, and the texture emulation's FP32
-// reference coordinates take more registers than the FP64 trilinear ones.
-// For the trilinear fused adjoint, 12 CTAs (M <= 2) measured as fast as 14
-// or 16 and 2 % faster than 10 on a 12-problem batch; 8 was slower.  For the
-// axis sampler's 3-material forward, 12 CTAs (80 registers, spills) ran a
-// 12-problem batch 2 % slower than 10 (96 registers, none).
+// (threads * minb)).  Forward, trilinear: 8 CTAs of 128 threads, 64
+// registers, the plain forward kernel's cap, for every material count: with
+// the texture handles in uniform registers the 3-material batch forward ran
+// the 3-material problems of the 48-problem batch 3.7 % slower than their
+// plain calls at this cap, and 9 % and 15 % slower at 6 and 5 CTAs (80 and
+// 96 registers).  Fused forward + adjoint (64-thread CTAs): it carries the
+// scatter's run accumulators on top of the march; 12 CTAs (M <= 2) measured
+// as fast as 14 or 16 and 2 % faster than 10 on a 12-problem batch, 8 was
+// slower.  The texture emulation's FP32 reference coordinates take more
+// registers than the FP64 trilinear ones.
 template <bool ADJOINT, int M, int MODE, bool AXIS>
 struct BatchBudget {
     static constexpr int minb = MODE == INTERP_TRILINEAR
-                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : (M <= 2 ? 8 : 5))
+                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : 8)
                                     : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 6 : 5));
 };
 
@@ -275,79 +276,98 @@ __global__ void __launch_bounds__(BatchShape<ADJOINT>::threads, BatchBudget<ADJO
 {
     constexpr int kThreads = BatchShape<ADJOINT>::threads, kWarps = BatchShape<ADJOINT>::warps;
     __shared__ float s_mu[CTFP_MAX_ENERGIES * M];
-    __shared__ long long s_unit;
     __shared__ float s_loss[kWarps];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // the current item and its unit range: the units a CTA takes mostly fall
-    // in one item, so the item search runs only when the item changes
-    int cached = -1;
-    long long c_begin = 0, c_end = 0;
+    // the current unit as thread 0 decoded it: item, first view, tile column
+    // and row, and whether the item changed.  Every thread re-reads these
+    // (volatile) where it needs them, so none of them is held in a register
+    // across a ray's march.
+    __shared__ int s_end, s_item, s_new, s_p, s_tu, s_tv;
+    // the current item and its unit range (thread 0): the units a CTA takes
+    // mostly fall in one item, so the item search runs only when the item
+    // changes
+    __shared__ int s_cached;
+    __shared__ long long s_cbegin, s_cend;
+    if (threadIdx.x == 0) {
+        s_cached = -1;
+        s_cbegin = s_cend = 0;
+    }
     for (;;) {
-        __syncthreads();  // the previous unit is done with s_mu, s_loss, s_unit
-        if (threadIdx.x == 0) s_unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
-        __syncthreads();
-        const long long unit = s_unit;
-        if (unit >= a.end) break;
-        const int k = (unit >= c_begin && unit < c_end) ? cached : find_item(a, unit);
-        const ItemDesc& it = a.items[k];
-        if (k != cached) {
-            for (int j = threadIdx.x; j < it.E * M; j += kThreads) s_mu[j] = it.mu[j];
-            cached = k;
-            c_begin = it.unit0;
-            c_end = it.unit0 + it.units;
-            __syncthreads();
-        }
-        const ItemTex<M> tx = item_tex<M, MODE, AXIS>(it);
-        // unit order within an item.  Forward: view group, then tile row, then
-        // tile column.  Adjoint: tile row, then view group, then tile column,
-        // so that the CTAs resident at any time work on one band of detector
-        // rows over many views: those rays cross a thin z-slab of the volume,
-        // whose accumulator cells then stay in L2.
-        const long long local = unit - it.unit0;
-        int p, tu, tv;
-        if (ADJOINT) {
-            const long long band_units = (long long)it.vgroups * it.tiles_u;
-            tv = (int)(local / band_units);
-            const int rem = (int)(local % band_units);
-            p = rem / it.tiles_u;
-            tu = rem % it.tiles_u;
-        } else {
-            const int tiles = it.tiles_u * it.tiles_v;
-            p = (int)(local / tiles);
-            const int t = (int)(local % tiles);
-            tv = t / it.tiles_u;
-            tu = t % it.tiles_u;
-        }
-        int u, v;
-        const int tile_u = 1 << a.tu_shift, tile_v = kThreads >> a.tu_shift;
-        if (AXIS && tile_v % 4 == 0 && tile_u <= kThreads / 4) {
-            // the axis sampler's lane quads run down 4 detector rows
-            const int q = threadIdx.x >> 2;
-            u = tu * tile_u + q % tile_u;
-            v = tv * tile_v + 4 * (q / tile_u) + (threadIdx.x & 3);
-        } else {
-            u = tu * tile_u + (threadIdx.x & (tile_u - 1));
-            v = tv * tile_v + (threadIdx.x >> a.tu_shift);
-        }
-        float loss = 0.f;
-        if (u < it.g.U && v < it.g.V) {
-            if (!MULTI) {
-                loss = process_ray<M, MODE, ADJOINT, AXIS>(it, tx, s_mu, p, v, u);
-            } else {
-                const int p_end = min((p + 1) * a.vpu, it.g.P);
-#pragma unroll 1
-                for (int pk = p * a.vpu; pk < p_end; pk++)
-                    loss += process_ray<M, MODE, ADJOINT, AXIS>(it, tx, s_mu, pk, v, u);
+        __syncthreads();  // the previous unit is done with s_mu, s_loss and the unit fields
+        if (threadIdx.x == 0) {
+            const long long unit = a.begin + (long long)atomicAdd(a.counter, 1ull);
+            s_end = unit >= a.end;
+            if (unit < a.end) {
+                const int cached = s_cached;
+                const int k = (unit >= s_cbegin && unit < s_cend) ? cached : find_item(a, unit);
+                const ItemDesc& it = a.items[k];
+                s_new = k != cached;
+                s_cached = k;
+                s_cbegin = it.unit0;
+                s_cend = it.unit0 + it.units;
+                // unit order within an item.  Forward: view group, then tile
+                // row, then tile column.  Adjoint: tile row, then view group,
+                // then tile column, so that the CTAs resident at any time work
+                // on one band of detector rows over many views: those rays
+                // cross a thin z-slab of the volume, whose accumulator cells
+                // then stay in L2.
+                const long long local = unit - it.unit0;
+                if (ADJOINT) {
+                    const long long band_units = (long long)it.vgroups * it.tiles_u;
+                    const int rem = (int)(local % band_units);
+                    s_tv = (int)(local / band_units);
+                    s_p = rem / it.tiles_u;
+                    s_tu = rem % it.tiles_u;
+                } else {
+                    const int tiles = it.tiles_u * it.tiles_v;
+                    const int t = (int)(local % tiles);
+                    s_p = (int)(local / tiles);
+                    s_tv = t / it.tiles_u;
+                    s_tu = t % it.tiles_u;
+                }
+                s_item = k;
             }
         }
-        if (ADJOINT && it.loss) {
-            for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
-            if (lane == 0) s_loss[warp] = loss;
+        __syncthreads();
+        if (*(volatile int*)&s_end) break;
+        const ItemDesc* const itp = a.items + *(volatile int*)&s_item;
+        if (*(volatile int*)&s_new) {
+            for (int j = threadIdx.x; j < itp->E * M; j += kThreads) s_mu[j] = itp->mu[j];
             __syncthreads();
-            if (threadIdx.x == 0) {
-                float t = 0.f;
-                for (int w = 0; w < kWarps; w++) t += s_loss[w];
-                atomicAdd(it.loss, t);
+        }
+        const ItemTex<M> tx = item_tex<M, MODE, AXIS>(*itp);
+        float loss = 0.f;
+#pragma unroll 1
+        for (int k = 0; k < (MULTI ? a.vpu : 1); k++) {
+            const ItemDesc& it = a.items[*(volatile int*)&s_item];
+            // this thread's ray within the unit's tile
+            const int tile_u = 1 << a.tu_shift, tile_v = kThreads >> a.tu_shift;
+            int du, dv;
+            if (AXIS && tile_v % 4 == 0 && tile_u <= kThreads / 4) {
+                // the axis sampler's lane quads run down 4 detector rows
+                const int q = threadIdx.x >> 2;
+                du = q % tile_u;
+                dv = 4 * (q / tile_u) + (threadIdx.x & 3);
+            } else {
+                du = threadIdx.x & (tile_u - 1);
+                dv = threadIdx.x >> a.tu_shift;
+            }
+            const int u = *(volatile int*)&s_tu * tile_u + du;
+            const int v = *(volatile int*)&s_tv * tile_v + dv;
+            const int pk = *(volatile int*)&s_p * (MULTI ? a.vpu : 1) + k;
+            if (u < it.g.U && v < it.g.V && pk < it.g.P) loss += process_ray<M, MODE, ADJOINT, AXIS>(it, tx, s_mu, pk, v, u);
+        }
+        if (ADJOINT) {
+            const ItemDesc& it = a.items[*(volatile int*)&s_item];
+            if (it.loss) {
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
+                if (lane == 0) s_loss[warp] = loss;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    float t = 0.f;
+                    for (int w = 0; w < kWarps; w++) t += s_loss[w];
+                    atomicAdd(it.loss, t);
+                }
             }
         }
     }

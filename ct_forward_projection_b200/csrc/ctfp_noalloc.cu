@@ -185,8 +185,17 @@ extern "C" ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_ma
     if (info.intNum <= 0 || info.intNum > 100000000)
         return nfail(CTFP_INVALID_ARG, "ctfp_forward_noalloc: intNum out of range");
 
+    // every call copies its host tables (spectrum, mu, the views'
+    // trigonometry) from pageable host memory, which a stream capture cannot
+    // record: refuse a capturing stream before anything is issued
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cap);
+    if (e != cudaSuccess) return nfail(CTFP_CUDA_ERROR, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+        return nfail(CTFP_UNSUPPORTED, "ctfp_forward_noalloc: the stream is capturing (its host-table copies cannot "
+                                       "be recorded in a graph)");
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return nfail(CTFP_CUDA_ERROR, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     unsigned char* scratch = nullptr;
     {

@@ -401,9 +401,12 @@ ctfp_status ctfp_backward_views(ctfp_plan* plan, const float* L_ckpt, const floa
  * projNum <= CTFP_NOALLOC_MAX_VIEWS, n_energies <= CTFP_MAX_ENERGIES,
  * n_materials <= CTFP_MAX_MATERIALS; larger sizes return CTFP_INVALID_ARG.
  * interp must be CTFP_INTERP_TRILINEAR or CTFP_INTERP_TEXEMU (the hardware
- * texture needs a cudaArray).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  That address is cached per device index for the life of the
+ * texture needs a cudaArray).  Every call copies its host tables (spectrum,
+ * mu, the views' trigonometry) from pageable host memory, which a CUDA graph
+ * capture cannot record: a call on a stream that is capturing returns
+ * CTFP_UNSUPPORTED and issues nothing.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress).  That address is cached per
+ * device index for the life of the
  * process: after the caller resets a device (cudaDeviceReset) the cached address
  * no longer names the array, so a process that resets a device must not call
  * this entry point on it again.  All calls on a device share the array and it

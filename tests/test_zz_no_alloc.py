@@ -143,3 +143,29 @@ def test_noalloc_without_grid_response_or_flat_field(interp):
             torch.cuda.synchronize()
             assert _rel(c["I"], ref["I"]) < RTOL
             assert _rel(c["A"], ref["IAbsorb"]) < RTOL
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """Each call copies its host tables from pageable memory, which a graph
+    capture cannot record: on a capturing stream the call returns
+    CTFP_UNSUPPORTED before it issues anything, and the capture stays valid."""
+    d = small_geometry(n=12, views=3, U=9, V=7)
+    vols = [torch.from_numpy(v).cuda() for v in random_volumes(d, 1, 990)]
+    S, mu, G, D = spectral_setup(d, 1, 5, 70, grid=False, det=False)
+    c = _prepare(d, vols, S, mu, G, D)
+    x = torch.zeros(4, device="cuda")
+    s = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        st = capi.lib().ctfp_forward_noalloc(C.byref(c["g"]), 1, 0, len(c["S"]), c["S"].ctypes.data_as(C.c_void_p),
+                                             c["mu"].ctypes.data_as(C.c_void_p), None, 0, None, C.c_float(1.0),
+                                             c["ptrs"], c["I"].data_ptr(), c["A"].data_ptr(), None,
+                                             C.c_void_p(s.cuda_stream))
+        x.add_(1.0)
+    assert st == capi.CTFP_UNSUPPORTED
+    assert "capturing" in capi.lib().ctfp_last_error_string().decode()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert float(x[0]) == 1.0
+    # outside the capture the same call runs
+    _noalloc(c, 0, 1.0, 0)
