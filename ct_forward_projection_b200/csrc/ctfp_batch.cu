@@ -256,14 +256,15 @@ __device__ __forceinline__ float process_ray(const ItemDesc& it, const ItemTex<M
 // the 3-material problems of the 48-problem batch 3.7 % slower than their
 // plain calls at this cap, and 9 % and 15 % slower at 6 and 5 CTAs (80 and
 // 96 registers).  Fused forward + adjoint (64-thread CTAs): it carries the
-// scatter's run accumulators on top of the march; 12 CTAs (M <= 2) measured
-// as fast as 14 or 16 and 2 % faster than 10 on a 12-problem batch, 8 was
-// slower.  The texture emulation's FP32 reference coordinates take more
-// registers than the FP64 trilinear ones.
+// scatter's run accumulators on top of the march; 14 CTAs (72 registers) for
+// M <= 2 and 12 (80) for more materials ran the 48-problem fused step 1.7 %
+// faster than 12 and 10 CTAs, and as fast as 16 (64 registers, spills).  The
+// texture emulation's FP32 reference coordinates take more registers than the
+// FP64 trilinear ones.
 template <bool ADJOINT, int M, int MODE, bool AXIS>
 struct BatchBudget {
     static constexpr int minb = MODE == INTERP_TRILINEAR
-                                    ? (ADJOINT ? (M <= 2 ? 12 : 10) : 8)
+                                    ? (ADJOINT ? (M <= 2 ? 14 : 12) : 8)
                                     : (ADJOINT ? (M <= 2 ? 10 : 8) : (M <= 2 ? 6 : 5));
 };
 
