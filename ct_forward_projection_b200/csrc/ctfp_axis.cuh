@@ -293,10 +293,10 @@ struct AxisScatter {
         for (int m = 0; m < M; m++) red_add_v4(acc[m] + k, sv[0] * g[m], sv[1] * g[m], sv[2] * g[m], sv[3] * g[m]);
     }
 
-    // The sample with footprint c and its 8 transposed weights w[k]
-    // (k = dz*4 + dy*2 + dx).
-    __device__ __forceinline__ void add(float4* const* __restrict__ acc, int nx, int ny, int nz, const Corner& c,
-                                        const float* w, const float* g)
+    // Moves the slots to footprint c (flushing a slot whose layer or base
+    // changes); returns the parity of c's lower layer.
+    __device__ __forceinline__ int step(float4* const* __restrict__ acc, int nx, int ny, int nz, const Corner& c,
+                                        const float* g)
     {
         const int lc = AX == 0 ? c.ix : c.iy, a = AX == 0 ? c.iy : c.ix, b = c.iz;
         const int par = lc & 1;
@@ -316,6 +316,35 @@ struct AxisScatter {
         h1 = e1;
         ca = a;
         cb = b;
+        return par;
+    }
+
+    // TRILINEAR: the sample's face weights straight from its axis weights:
+    // the four in-layer products (a, b), (a + 1, b), (a, b + 1), (a + 1, b + 1)
+    // times the layer weight of each slot (the lower layer's in the slot of
+    // its parity).  The same products as the 8 trilinear weights, with the
+    // layer axis's weight applied last.
+    __device__ __forceinline__ void add_trilinear(float4* const* __restrict__ acc, int nx, int ny, int nz,
+                                                  const Corner& c, const float* g)
+    {
+        const int par = step(acc, nx, ny, nz, c, g);
+        const float ua = AX == 0 ? c.uy : c.ux, wa = AX == 0 ? c.wy : c.wx;
+        const float wl = AX == 0 ? c.ux : c.uy, wh = AX == 0 ? c.wx : c.wy;
+        const float w0 = par ? wh : wl, w1 = par ? wl : wh;
+        const float p[4] = {ua * c.uz, wa * c.uz, ua * c.wz, wa * c.wz};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            s0[j] = fmaf(p[j], w0, s0[j]);
+            s1[j] = fmaf(p[j], w1, s1[j]);
+        }
+    }
+
+    // The sample with footprint c and its 8 transposed weights w[k]
+    // (k = dz*4 + dy*2 + dx).
+    __device__ __forceinline__ void add(float4* const* __restrict__ acc, int nx, int ny, int nz, const Corner& c,
+                                        const float* w, const float* g)
+    {
+        const int par = step(acc, nx, ny, nz, c, g);
         constexpr int lb = AX == 0 ? 1 : 2;  // the layer bit of k
         constexpr int ab = AX == 0 ? 2 : 1;  // the in-layer axis bit of k
 #pragma unroll
@@ -364,16 +393,24 @@ __device__ __forceinline__ void scatter_ray_axis(const GeomParams& gp, float4* c
         AxisScatter<M, 0> run;
         for (int i = s.i0; i < s.i1; i++) {
             const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
-            corner_weights<MODE>(c, w);
-            run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+            if (MODE == INTERP_TRILINEAR) {
+                run.add_trilinear(acc, gp.nx, gp.ny, gp.nz, c, g);
+            } else {
+                corner_weights<MODE>(c, w);
+                run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+            }
         }
         run.finish(acc, gp.nx, gp.ny, gp.nz, g);
     } else {
         AxisScatter<M, 1> run;
         for (int i = s.i0; i < s.i1; i++) {
             const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
-            corner_weights<MODE>(c, w);
-            run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+            if (MODE == INTERP_TRILINEAR) {
+                run.add_trilinear(acc, gp.nx, gp.ny, gp.nz, c, g);
+            } else {
+                corner_weights<MODE>(c, w);
+                run.add(acc, gp.nx, gp.ny, gp.nz, c, w, g);
+            }
         }
         run.finish(acc, gp.nx, gp.ny, gp.nz, g);
     }

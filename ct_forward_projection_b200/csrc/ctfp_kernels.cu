@@ -285,8 +285,10 @@ __global__ void __launch_bounds__(256) k_spectral_from_L(const MarchParams prm)
 // views.  The rays of a row band cross a thin z-slab of the volume (the cone
 // angle is small), so the accumulator cells they reduce into stay in L2; with
 // views outermost every view would sweep the whole accumulator through DRAM.
+// Register cap for 4 CTAs of 256 threads (64 registers, ~40 B of spills): the
+// poly_grid_256 adjoint 0.8 ms faster than at 3 CTAs (76 registers, none).
 template <int M, int MODE, bool FROM_GL>
-__global__ void __launch_bounds__(256, 3) k_backward(const MarchParams prm)
+__global__ void __launch_bounds__(256, 4) k_backward(const MarchParams prm)
 {
     extern __shared__ float s_mu[];
     if (!FROM_GL) load_mu(s_mu, prm.mu, prm.E * M);
