@@ -105,6 +105,7 @@ _SIGNATURES = {
     "ctfp_batch_get_shapes": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_int32)]),
     "ctfp_batch_set_views": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "ctfp_check_division": (C.c_int, [C.c_int32, C.c_float, C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
     "ctfp_batch_get_views": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ctfp_last_error_string": (C.c_char_p, []),
     "ctfp_version": (C.c_char_p, []),

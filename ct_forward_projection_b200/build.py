@@ -60,11 +60,14 @@ def build_lib(force: bool = False) -> str:
     objdir = os.path.join(ROOT, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
-    # the translation units compile independently: in parallel, largest first
+    # the translation units compile independently: in parallel, largest first.
+    # Whole-program device code per unit (-c): no device function or variable
+    # crosses units, and relocatable device code (-dc) ran the forward march
+    # 2 % slower.
     from concurrent.futures import ThreadPoolExecutor
     jobs = sorted(zip(srcs, objs), key=lambda so: -os.path.getsize(so[0]))
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
-        for f in [ex.submit(_run, [NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-dc", s, "-o", o]) for s, o in jobs]:
+        for f in [ex.submit(_run, [NVCC, *NVCC_FLAGS, "-I", INCLUDE, "-c", s, "-o", o]) for s, o in jobs]:
             f.result()
     _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
     return LIB

@@ -494,6 +494,7 @@ ctfp_status ctfp_plan_create(const ctfp_geometry* g, int32_t n_materials, int32_
     gp.sod = g->sod; gp.sdd = g->sdd; gp.FOVR = info.FOVR; gp.dx = info.dx;
     gp.pHalfX = info.pHalfX; gp.pHalfY = info.pHalfY; gp.pHalfZ = info.pHalfZ;
     gp.pSizeX = info.pSizeX; gp.pSizeY = info.pSizeY; gp.pSizeZ = info.pSizeZ;
+    gp.rpSizeX = 1.0f / info.pSizeX; gp.rpSizeY = 1.0f / info.pSizeY; gp.rpSizeZ = 1.0f / info.pSizeZ;
     std::vector<double2> trig((size_t)g->projNum);
     std::vector<float2> trigf((size_t)g->projNum);
     for (int64_t k = 0; k < g->projNum; k++) {

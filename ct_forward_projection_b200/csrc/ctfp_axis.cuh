@@ -43,16 +43,6 @@ struct OccView {
 // layer indices, so a footprint overhanging the volume reads zeros there with
 // no test.
 
-// In-layer bilinear value of one gather q (tld4 order: x = (a, b+1),
-// y = (a+1, b+1), z = (a+1, b), w = (a, b)) with weights (ua, wa) on the
-// in-layer axis a and (ub, wb) on z.
-__device__ __forceinline__ float bilinear_quad(const float4& q, float ua, float wa, float ub, float wb)
-{
-    const float r0 = fmaf(q.z, wa, q.w * ua);
-    const float r1 = fmaf(q.y, wa, q.x * ua);
-    return fmaf(r1, wb, r0 * ub);
-}
-
 // The gathers one ray holds: the layers in slot 0 (even) and slot 1 (odd)
 // and their in-layer base; the sentinel layer matches no footprint (bases are
 // >= -2).  fetch() takes the next footprint (lower layer lc, in-layer base
@@ -146,15 +136,20 @@ __device__ __forceinline__ void march_ray_axis(const GeomParams& g, const cudaTe
             for (int m = 0; m < M; m++) q1[m] = gather_layer_cond(tx[m], e1 + 1, fa, fb);
         }
         if (MODE == INTERP_TRILINEAR) {
-            // weights of the lower and upper layer, assigned to the slots by parity
+            // weights of the lower and upper layer, assigned to the slots by
+            // parity; each gather's in-layer value as a dot product with the
+            // four in-layer weight products (shared by the materials and both
+            // slots; tld4 order: x = (a, b+1), y = (a+1, b+1), z = (a+1, b),
+            // w = (a, b)), the slots' layer weights folded into the block sum
             const float wl = AX == 0 ? c.ux : c.uy, wh = AX == 0 ? c.wx : c.wy;
             const float w0 = par ? wh : wl, w1 = par ? wl : wh;
             const float ua = AX == 0 ? c.uy : c.ux, wa = AX == 0 ? c.wy : c.wx;
+            const float p00 = ua * c.uz, p10 = wa * c.uz, p01 = ua * c.wz, p11 = wa * c.wz;
 #pragma unroll
             for (int m = 0; m < M; m++) {
-                const float s0 = bilinear_quad(q0[m], ua, wa, c.uz, c.wz);
-                const float s1 = bilinear_quad(q1[m], ua, wa, c.uz, c.wz);
-                blk[m] += fmaf(s1, w1, s0 * w0);
+                const float s0 = fmaf(q0[m].y, p11, fmaf(q0[m].x, p01, fmaf(q0[m].z, p10, q0[m].w * p00)));
+                const float s1 = fmaf(q1[m].y, p11, fmaf(q1[m].x, p01, fmaf(q1[m].z, p10, q1[m].w * p00)));
+                blk[m] = fmaf(s1, w1, fmaf(s0, w0, blk[m]));
             }
         } else {
             // the texture unit's 8 weights (k = dz*4 + dy*2 + dx); the layer

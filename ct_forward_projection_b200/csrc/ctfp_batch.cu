@@ -178,7 +178,7 @@ __device__ __forceinline__ void batch_march(const ItemDesc& it, const ItemTex<M>
     if (MODE == INTERP_TEXTURE) {
 #pragma unroll 2
         for (int i = s.i0; i < s.i1; i++) {
-            const float3 x = ref32_coords(it.g, r, i);
+            const float3 x = ref32_coords<false>(it.g, r, i);
 #pragma unroll
             for (int m = 0; m < M; m++) kahan_add(acc[m], cmp[m], tex3D<float>(tx.t[m], x.x, x.y, x.z));
         }

@@ -25,6 +25,29 @@ namespace {
 
 constexpr int kDim = 32, kLayers = 8, kIters = 2048;
 
+// Compares div_rn_recip(x, y, r) with the IEEE division x / y bit for bit on
+// n pseudo-random x per thread block sweep: x = +-(1 + m 2^-23) 2^e with a
+// uniformly random 23-bit m and e in [-20, 20], from a SplitMix64 stream.
+__global__ void __launch_bounds__(256) k_check_division(float y, float r, long long n, unsigned long long seed,
+                                                        unsigned long long* mismatches)
+{
+    unsigned long long bad = 0;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(k + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        const unsigned m = (unsigned)z & 0x7FFFFFu;
+        const int e = (int)((z >> 23) % 41ull) - 20;
+        const unsigned sign = (unsigned)(z >> 63) << 31;
+        const float x = __uint_as_float(sign | ((unsigned)(e + 127) << 23) | m);
+        const float q = __fdiv_rn(x, y);
+        const float d = div_rn_recip(x, y, r);
+        bad += __float_as_uint(q) != __float_as_uint(d);
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+
 // One voxel-sample per iteration and thread: two gathers (layers l, l + 1).
 __global__ void __launch_bounds__(256) k_peak_gather(cudaTextureObject_t t, float* out)
 {
@@ -133,4 +156,34 @@ extern "C" ctfp_status ctfp_sampler_peak(int32_t device, int32_t kind, double* v
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
     if (rs != CTFP_OK) set_last_error(where);
     return rs;
+}
+
+extern "C" ctfp_status ctfp_check_division(int32_t device, float divisor, int64_t n, uint64_t seed,
+                                           int64_t* mismatches)
+{
+    if (!mismatches || n < 0 || !(divisor > 0.f) || divisor > 1e30f) {
+        set_last_error("ctfp_check_division: needs a positive finite divisor, n >= 0 and an output");
+        return CTFP_INVALID_ARG;
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != device) cudaSetDevice(device);
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(unsigned long long));
+    const float r = 1.0f / divisor;  // the reciprocal the plans store (rpSize)
+    if (e == cudaSuccess) {
+        k_check_division<<<148 * 8, 256>>>(divisor, r, (long long)n, (unsigned long long)seed, d);
+        e = cudaGetLastError();
+    }
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("ctfp_check_division: ") + cudaGetErrorString(e));
+        return CTFP_CUDA_ERROR;
+    }
+    *mismatches = (int64_t)h;
+    return CTFP_OK;
 }

@@ -75,7 +75,7 @@ __device__ __forceinline__ void march_ray(const MarchParams& prm, int p, int v, 
         const RayRef32 r = ray_ref32(prm.g, p, v, u);
 #pragma unroll 2
         for (int i = s.i0; i < s.i1; i++) {
-            const float3 x = ref32_coords(prm.g, r, i);
+            const float3 x = ref32_coords<false>(prm.g, r, i);
             // with empty-space skipping: the unit's own footprint (base texel
             // of its fixed-point coordinate) in an all-zero brick filters to 0
             if (SAMPLER == SAMPLER_LAYERED_SKIP && !footprint_occupied(prm, corner_tex(x))) continue;

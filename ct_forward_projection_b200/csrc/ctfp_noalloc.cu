@@ -244,6 +244,7 @@ extern "C" ctfp_status ctfp_forward_noalloc(const ctfp_geometry* g, int32_t n_ma
     gp.sod = g->sod; gp.sdd = g->sdd; gp.FOVR = info.FOVR; gp.dx = info.dx;
     gp.pHalfX = info.pHalfX; gp.pHalfY = info.pHalfY; gp.pHalfZ = info.pHalfZ;
     gp.pSizeX = info.pSizeX; gp.pSizeY = info.pSizeY; gp.pSizeZ = info.pSizeZ;
+    gp.rpSizeX = 1.0f / info.pSizeX; gp.rpSizeY = 1.0f / info.pSizeY; gp.rpSizeZ = 1.0f / info.pSizeZ;
     gp.trig = d_trig;
     gp.trigf = d_trigf;
     for (int m = 0; m < M; m++) q.vol[m] = volumes[m];

@@ -275,12 +275,26 @@ ctfp_status ctfp_line_integrals_adjoint(ctfp_plan* plan, const float* gL, float*
  * occupancy, with the march's warp shape.  Writes voxel-samples per second. */
 ctfp_status ctfp_sampler_peak(int32_t device, int32_t kind, double* voxel_samples_per_s);
 
+/* No counterpart in the reference.  The texture-emulation mode's sample
+ * coordinates divide by the voxel size as the reference does, with the
+ * quotient formed from the plan's FP32 reciprocal of the divisor and two
+ * exact-remainder correction steps instead of an IEEE division.  This check runs that
+ * arithmetic on n pseudo-random dividends (both signs, magnitudes 2^-20 to
+ * 2^21, seeded) against the device's IEEE division by `divisor` and writes the
+ * number of results that differ in any bit (0 expected). */
+ctfp_status ctfp_check_division(int32_t device, float divisor, int64_t n, uint64_t seed, int64_t* mismatches);
+
 /* ---- launch-shape autotuner ------------------------------------------------
  * No counterpart in the reference (fixed 8 x 8 x 8 blocks,
  * Source/CUDAFun/CBCTPolyProjGPU.cuh:22-24).  Times candidate launch shapes of
  * the fused forward (tiles 8 x 8 ... 64 x 4, 2-4 CTAs per SM, 1-4 views per CTA)
  * on n_sample_views views (0: 16) in four chunks spread round the rotation, and
- * sets the fastest on the plan (as ctfp_plan_set_launch_shape).  I and IAbsorb
+ * sets the fastest on the plan (as ctfp_plan_set_launch_shape).  A chunk of a
+ * few waves of CTAs ends in a partial wave that weighs more for CTAs of more
+ * views, so short samples lean towards 1 view per CTA: on the 256^3 two-material
+ * 360-view workload 16 views per chunk picked 1 view per CTA where 2 run the
+ * whole forward 2.7 % faster; give it every view when the tuning time (about
+ * 36 forwards of the sample) allows.  I and IAbsorb
  * are full-size output buffers as for ctfp_forward; their contents are
  * undefined afterwards.  Synchronises the stream.  Results are cached per
  * process by geometry, materials, sampler, energies and device name, and in the

@@ -607,3 +607,24 @@ def test_axis_gather_count_reuse_on_a_fine_march(cuda_ok):
         pr.set_sampler("axis")
         g = pr.axis_gather_count()
     assert g < 0.3
+
+
+def test_reciprocal_division_is_the_ieee_division(cuda_ok):
+    """The texture emulation's coordinates divide by the voxel size through the
+    plan's FP32 reciprocal and two exact-remainder correction steps; every
+    quotient must equal the IEEE division bit for bit (the reference divides),
+    for the voxel sizes of the benchmark workloads, divisors whose mantissa
+    sits at either end of its binade, and seeded random divisors."""
+    import ctypes as C
+
+    from ct_forward_projection_b200 import _capi as capi
+    fixed = [0.5, 0.4, 0.8, 1.0, 0.75, 2.5, 0.3, 1.0 / 3.0, 0.7, 0.1, 0.390625, 1.2, 0.123456,
+             float(np.nextafter(np.float32(1.0), np.float32(0))), float(np.nextafter(np.float32(1.0), np.float32(2))),
+             float(np.nextafter(np.float32(2.0), np.float32(0))), 1.5, 3.0, 7.0, 0.0625]
+    rng = np.random.RandomState(17)
+    rand = [float(np.float32(x)) for x in np.exp(rng.uniform(np.log(0.02), np.log(8.0), 200))]
+    for k, y in enumerate(fixed + rand):
+        bad = C.c_int64(-1)
+        capi.call("ctfp_check_division", 0, C.c_float(y), 4_000_000 if k < len(fixed) else 500_000, 1000 + k,
+                  C.byref(bad))
+        assert bad.value == 0, (y, bad.value)
