@@ -318,6 +318,8 @@ def main():
                     help="where the software interp modes read corners")
     ap.add_argument("--batch-items", type=int, default=48,
                     help="problems in the uneven batch leg (0 skips it)")
+    ap.add_argument("--no-batch-autotune", action="store_true",
+                    help="batch leg with the default work units (no ctfp_batch_autotune)")
     ap.add_argument("--batch-passes", type=int, default=3,
                     help="timed passes per arm of the batch leg (after one warm-up pass; arms interleaved)")
     ap.add_argument("--launch-shape", default=None,
@@ -804,8 +806,13 @@ def batch_leg(args, ws, rank, local, stream):
         pr.forward(v, out=o)
         targets.append(o["I"] * torch.exp(0.05 * torch.randn(o["I"].shape, device=dev, generator=gen)))
     b = Batch(prs)
-    # the work-unit ray tile, tuned on the fused kernels (untimed)
-    unit_shape = b.autotune(vols, targets)
+    # the work units, tuned for each kind of call (untimed)
+    if args.no_batch_autotune:
+        sh = b.shapes()
+        unit_shape = {"tile_u": sh["fwd_adjoint"][0], "tile_v": sh["fwd_adjoint"][1], "views": sh["views"][1],
+                      "fwd_tile_u": sh["fwd"][0], "fwd_tile_v": sh["fwd"][1], "fwd_views": sh["views"][0]}
+    else:
+        unit_shape = b.autotune(vols, targets)
     b_outs = [{"I": torch.empty_like(o["I"]), "IAbsorb": torch.empty_like(o["I"])} for o in outs]
     b_I = [torch.empty_like(o["I"]) for o in outs]
     loss_b = torch.zeros(len(prs), device=dev)

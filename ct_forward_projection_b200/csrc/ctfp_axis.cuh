@@ -374,9 +374,10 @@ __device__ __forceinline__ void corner_weights(const Corner& c, float* w)
 // The adjoint scatter of one ray: the transposed weights of the march's
 // samples (FP64 coordinates for TRILINEAR, the reference's FP32 coordinates
 // and the texture unit's weights otherwise) into the face accumulators of the
-// view's march axis, scaled by g[m] = dLoss/dL_m times dx.  The sample loops
-// are unrolled by 2: the poly_grid_256 forward + adjoint step ran 1.0 ms and
-// the fused step 1.6 ms faster than with them rolled.
+// view's march axis, scaled by g[m] = dLoss/dL_m times dx.  For M <= 2 the
+// sample loops are unrolled by 2: the poly_grid_256 forward + adjoint step ran
+// 1.0 ms and the fused step 1.6 ms faster than with them rolled; the
+// 4-material adjoint of large_4mat_512 ran 2.6 % slower unrolled.
 template <int M, int MODE>
 __device__ __forceinline__ void scatter_ray_axis(const GeomParams& gp, float4* const* __restrict__ acc, int p, int v,
                                                  int u, const float* g, bool axis_x)
@@ -388,7 +389,7 @@ __device__ __forceinline__ void scatter_ray_axis(const GeomParams& gp, float4* c
     float w[8];
     if (axis_x) {
         AxisScatter<M, 0> run;
-#pragma unroll 2
+#pragma unroll(M <= 2 ? 2 : 1)
         for (int i = s.i0; i < s.i1; i++) {
             const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
             if (MODE == INTERP_TRILINEAR) {
@@ -401,7 +402,7 @@ __device__ __forceinline__ void scatter_ray_axis(const GeomParams& gp, float4* c
         run.finish(acc, gp.nx, gp.ny, gp.nz, g);
     } else {
         AxisScatter<M, 1> run;
-#pragma unroll 2
+#pragma unroll(M <= 2 ? 2 : 1)
         for (int i = s.i0; i < s.i1; i++) {
             const Corner c = axis_corner<MODE>(gp, r, i, cx, cy, cz, s);
             if (MODE == INTERP_TRILINEAR) {
