@@ -7,9 +7,10 @@
 // (2, 3, 4 CTAs per SM) with 2 views per CTA; stage 2 times the three best
 // with 1, 2 and 4 views per CTA.  Each candidate runs the fused forward over
 // four chunks of views spread round the rotation (the sampling pattern changes
-// with the angle), once to warm up and twice timed with CUDA events; the
-// fastest total wins.  Results are cached per process under a key of the
-// geometry, materials, sampler, energies and device name, and optionally in
+// with the angle) launched concurrently on four streams, once to warm up and
+// twice timed with CUDA events; the fastest total wins.  Results are cached
+// per process under a key of the geometry, materials, sampler, energies and
+// device name, and optionally in
 // the text file named by CTFP_TUNE_CACHE (one "key tile_u tile_v views
 // min_ctas ms" line per entry), which later processes read.
 #include <algorithm>
@@ -107,21 +108,55 @@ bool valid_shape(const LaunchShape& s)
            t * s.min_ctas <= 2048;
 }
 
+// Streams and events of one tuning run: the view chunks of a candidate run
+// concurrently, one per stream, so the sample ends in one partial wave of
+// CTAs rather than one per chunk (a chunk of a few waves run alone ends in a
+// partial wave that weighs more for CTAs of more views, which made short
+// samples favour 1 view per CTA).
+struct ChunkStreams {
+    cudaStream_t s[4] = {};
+    cudaEvent_t fork = nullptr, join[4] = {};
+    ~ChunkStreams()
+    {
+        for (cudaStream_t x : s)
+            if (x) cudaStreamDestroy(x);
+        for (cudaEvent_t x : join)
+            if (x) cudaEventDestroy(x);
+        if (fork) cudaEventDestroy(fork);
+    }
+    cudaError_t create()
+    {
+        cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        for (int k = 0; k < 4 && e == cudaSuccess; k++) {
+            e = cudaStreamCreateWithFlags(&s[k], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming);
+        }
+        return e;
+    }
+};
+
 // Total time of one candidate over the view chunks (ms), or a negative value
 // on a launch error.
 float time_shape(const MarchParams& base, int M, int interp, int sampler, const LaunchShape& ls,
                  const std::vector<std::pair<int, int>>& chunks, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t st,
-                 int reps)
+                 ChunkStreams& cs, int reps)
 {
     auto run_all = [&]() -> cudaError_t {
-        for (const auto& c : chunks) {
+        // every chunk stream starts after the work already on st, and st
+        // continues after all of them
+        cudaError_t e = cudaEventRecord(cs.fork, st);
+        for (size_t k = 0; k < chunks.size() && e == cudaSuccess; k++) {
+            cudaStream_t sk = cs.s[k % 4];
+            e = cudaStreamWaitEvent(sk, cs.fork, 0);
             MarchParams prm = base;
-            prm.view0 = c.first;
-            prm.n_views = c.second;
-            cudaError_t e = launch_forward(prm, M, interp, sampler, true, ls, st);
-            if (e != cudaSuccess) return e;
+            prm.view0 = chunks[k].first;
+            prm.n_views = chunks[k].second;
+            if (e == cudaSuccess) e = launch_forward(prm, M, interp, sampler, true, ls, sk);
+            if (e == cudaSuccess) e = cudaEventRecord(cs.join[k % 4], sk);
         }
-        return cudaSuccess;
+        for (size_t k = 0; k < chunks.size() && k < 4 && e == cudaSuccess; k++)
+            e = cudaStreamWaitEvent(st, cs.join[k], 0);
+        return e;
     };
     if (run_all() != cudaSuccess) return -1.f;
     if (cudaEventRecord(e0, st) != cudaSuccess) return -1.f;
@@ -142,7 +177,7 @@ extern "C" ctfp_status ctfp_plan_autotune(ctfp_plan* p, const float* const* volu
     if (!volumes || !I) return tfail(CTFP_INVALID_ARG, "volumes and I are required");
     if (plan_energies(p) < 1) return tfail(CTFP_NOT_READY, "spectral tables not set");
     const GeomParams& g = plan_geom(p);
-    int n = n_sample_views > 0 ? n_sample_views : 16;
+    int n = n_sample_views > 0 ? n_sample_views : 64;
     n = std::min(n, g.P);
     const std::string key = cache_key(p, n);
     {
@@ -181,9 +216,11 @@ extern "C" ctfp_status ctfp_plan_autotune(ctfp_plan* p, const float* const* volu
     base.IAbs = IAbsorb;
     const int M = plan_materials(p), interp = plan_interp(p), sampler = plan_sampler(p);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ChunkStreams cs;
     Entry best{plan_shape(p), -1.f};
-    if (rs == CTFP_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
-        rs = tfail(CTFP_CUDA_ERROR, "cudaEventCreate failed");
+    if (rs == CTFP_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+                          cs.create() != cudaSuccess))
+        rs = tfail(CTFP_CUDA_ERROR, "cudaEventCreate / cudaStreamCreate failed");
     if (rs == CTFP_OK) {
         static const int tiles[][2] = {{16, 8}, {32, 4}, {8, 16}, {64, 2}, {16, 16}, {32, 8}, {8, 32}, {64, 4},
                                        {8, 8},  {16, 4}};
@@ -192,7 +229,7 @@ extern "C" ctfp_status ctfp_plan_autotune(ctfp_plan* p, const float* const* volu
             for (int minb = 2; minb <= 4; minb++) {
                 LaunchShape ls{t[0], t[1], 2, minb};
                 if (!valid_shape(ls)) continue;
-                const float ms = time_shape(base, M, interp, sampler, ls, chunks, e0, e1, st, 2);
+                const float ms = time_shape(base, M, interp, sampler, ls, chunks, e0, e1, st, cs, 2);
                 if (ms < 0.f) {
                     rs = tfail(CTFP_CUDA_ERROR, std::string("autotune launch: ") + cudaGetErrorString(cudaGetLastError()));
                     break;
@@ -207,7 +244,7 @@ extern "C" ctfp_status ctfp_plan_autotune(ctfp_plan* p, const float* const* volu
                 for (int vpc : {1, 4}) {
                     LaunchShape ls = stage1[i].shape;
                     ls.views_per_cta = vpc;
-                    const float ms = time_shape(base, M, interp, sampler, ls, chunks, e0, e1, st, 2);
+                    const float ms = time_shape(base, M, interp, sampler, ls, chunks, e0, e1, st, cs, 2);
                     if (ms < 0.f) {
                         rs = tfail(CTFP_CUDA_ERROR, "autotune launch failed");
                         break;

@@ -177,7 +177,7 @@ class Projector:
     def set_launch_shape(self, tile_u: int, tile_v: int, views_per_cta: int = 1, min_ctas_per_sm: int = 2) -> None:
         call("ctfp_plan_set_launch_shape", self._h, tile_u, tile_v, views_per_cta, min_ctas_per_sm)
 
-    def autotune(self, volumes: Sequence, n_sample_views: int = 16, stream=None) -> dict:
+    def autotune(self, volumes: Sequence, n_sample_views: int = 64, stream=None) -> dict:
         """ctfp_plan_autotune: times launch shapes on a sample of views and
         sets the fastest; returns it with its time and whether it was cached."""
         import torch

@@ -288,13 +288,13 @@ ctfp_status ctfp_check_division(int32_t device, float divisor, int64_t n, uint64
  * No counterpart in the reference (fixed 8 x 8 x 8 blocks,
  * Source/CUDAFun/CBCTPolyProjGPU.cuh:22-24).  Times candidate launch shapes of
  * the fused forward (tiles 8 x 8 ... 64 x 4, 2-4 CTAs per SM, 1-4 views per CTA)
- * on n_sample_views views (0: 16) in four chunks spread round the rotation, and
- * sets the fastest on the plan (as ctfp_plan_set_launch_shape).  A chunk of a
- * few waves of CTAs ends in a partial wave that weighs more for CTAs of more
- * views, so short samples lean towards 1 view per CTA: on the 256^3 two-material
- * 360-view workload 16 views per chunk picked 1 view per CTA where 2 run the
- * whole forward 2.7 % faster; give it every view when the tuning time (about
- * 36 forwards of the sample) allows.  I and IAbsorb
+ * on n_sample_views views (0: 64) in four chunks spread round the rotation,
+ * run concurrently, and sets the fastest on the plan (as
+ * ctfp_plan_set_launch_shape).  The sample ends in a partial wave of CTAs that
+ * weighs more for CTAs of more views, so short samples lean towards 1 view per
+ * CTA: on the 256^3 two-material 360-view workload 64 sample views pick what
+ * all 360 pick (2 views per CTA), 16 pick 1 view per CTA, 5 % slower on the
+ * whole forward.  Tuning takes about 36 forwards of the sample.  I and IAbsorb
  * are full-size output buffers as for ctfp_forward; their contents are
  * undefined afterwards.  Synchronises the stream.  Results are cached per
  * process by geometry, materials, sampler, energies and device name, and in the
