@@ -510,6 +510,14 @@ __device__ __forceinline__ void spectral(const float* s_mu, int E, const float* 
     float sI[4] = {0.f, 0.f, 0.f, 0.f}, sA[4] = {0.f, 0.f, 0.f, 0.f};
     const float* Wp = W + pix;
     int e = 0;
+    // 8 energies per step (8 table loads in flight; 0.5 % of the 256^3
+    // two-material forward against 4), accumulator k & 3 taking energy e + k:
+    // every accumulator sums the same energies in the same order as with
+    // steps of 4, so the sums do not change
+    for (; e + 8 <= E; e += 8) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) spectral_term<M>(s_mu, e + k, Wp, npix, L, sI[k & 3], sA[k & 3]);
+    }
     for (; e + 4 <= E; e += 4) {
 #pragma unroll
         for (int k = 0; k < 4; k++) spectral_term<M>(s_mu, e + k, Wp, npix, L, sI[k], sA[k]);
@@ -547,6 +555,11 @@ __device__ __forceinline__ void spectral_adjoint(const float* s_mu, int E, const
     for (int m = 0; m < M; m++) S[m] = 0.f;
     const float* Wp = W + pix;
     int e = 0;
+    // the steps of spectral(): the same order for sI, and S in energy order
+    for (; e + 8 <= E; e += 8) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) spectral_adjoint_term<M>(s_mu, e + k, Wp, npix, L, sI[k & 3], S);
+    }
     for (; e + 4 <= E; e += 4) {
 #pragma unroll
         for (int k = 0; k < 4; k++) spectral_adjoint_term<M>(s_mu, e + k, Wp, npix, L, sI[k], S);
